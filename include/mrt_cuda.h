@@ -1,0 +1,240 @@
+/*
+ * mrt_cuda.h - C ABI of the B200 render path for MobileRT (MobileRayTracer).
+ *
+ * Plain C types only: pointers, sizes and POD structs.  Every entry point returns an MRT_* status
+ * code; the text of the last failure on a context is available from mrt_context_error().  No call
+ * falls back to the CPU: if the CUDA device or the kernels are unavailable the call fails.
+ *
+ * Which reference interface each entry point replaces (paths inside the MobileRayTracer checkout):
+ *   mrt_scene_create      Scene{triangles_, spheres_, planes_, materials_, lights_} filled by the caller
+ *                         (app/MobileRT/Scene.hpp:23-27, filled in app/Scenes/Scenes.cpp:7-314 or
+ *                         app/Components/ObjectLoaders/OBJLoader.cpp:68-248)
+ *   mrt_scene_build       Shader::initializeAccelerators(Camera*)   (app/MobileRT/Shader.cpp:31-122)
+ *                         -> Naive<T>, RegularGrid<T>, BVH<T> constructors
+ *   mrt_trace_closest     Shader::rayTrace's accelerator part: planes -> spheres -> triangles -> lights
+ *                         (app/MobileRT/Shader.cpp:124-150; BVH<T>::trace BVH.hpp:158-213,
+ *                         RegularGrid<T>::trace RegularGrid.hpp:157-337, Naive<T>::trace Naive.hpp:56-63)
+ *   mrt_trace_any         Shader::shadowTrace(ray, dist)             (app/MobileRT/Shader.cpp:162-187)
+ *   mrt_render            Renderer::renderFrame(bitmap, numThreads, stride)
+ *                         (app/MobileRT/Renderer.cpp:31-59, renderScene :67-116) with the shader's
+ *                         shade() (app/Components/Shaders/{NoShadows,Whitted,PathTracer}.cpp)
+ *   mrt_render_stop       Renderer::stopRender()                     (app/MobileRT/Renderer.cpp:61-65)
+ *   mrt_render_progress   Renderer::getSample()                      (app/MobileRT/Renderer.cpp:118-120)
+ */
+#ifndef MRT_CUDA_H
+#define MRT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------- */
+#define MRT_OK 0
+#define MRT_ERR_ARG 1        /* invalid argument (null pointer, size out of range, bad enum) */
+#define MRT_ERR_OOM 2        /* device allocation failed */
+#define MRT_ERR_CUDA 3       /* a CUDA runtime call failed; the context may be unusable */
+#define MRT_ERR_LIMIT 4      /* a traversal step cap or queue capacity was exceeded */
+#define MRT_ERR_CANCELLED 5  /* mrt_render_stop() was called while a render was in flight */
+#define MRT_ERR_STATE 6      /* call out of order (e.g. trace before mrt_scene_build) */
+
+/* ---- enums (reference integer codes are kept where the reference has them) ----------------- */
+/* Shader::Accelerator (app/MobileRT/Shader.hpp:34-38) */
+#define MRT_ACCEL_NAIVE 0
+#define MRT_ACCEL_REGULAR_GRID 1
+#define MRT_ACCEL_BVH 2
+
+/* BVH flavour.  REFERENCE rebuilds the reference tree (unsorted top-down SAH, leaf <= 2,
+ * BVH.hpp:87-155,273-311) and walks it with the reference slab test in the reference order, so its
+ * results equal BVH<T>::trace bit for bit, including the slab test's rejections.  FAST builds a
+ * Morton-ordered tree on the device and walks it front to back with a conservative slab test; its
+ * closest hit is the exact closest hit (= Naive<T>), ties resolved to the lowest primitive index. */
+#define MRT_BVH_FAST 0
+#define MRT_BVH_REFERENCE 1
+
+/* RegularGrid cell addressing.  The reference fills cells at x + y*G + z*G*G
+ * (RegularGrid.hpp:134-138) but reads them at X + (Y << s) + (Z << 2s), s = bitCounter(G) - 1
+ * (RegularGrid.hpp:237-241); both agree only for power-of-two G.  REFERENCE keeps that pair of
+ * formulas (bit-exact with the reference at any G); LINEAR reads with the fill formula. */
+#define MRT_GRID_INDEX_REFERENCE 0
+#define MRT_GRID_INDEX_LINEAR 1
+
+/* c_wrapper.cpp:444-486 shader codes: 1 Whitted, 2 PathTracer, default NoShadows */
+#define MRT_SHADER_NOSHADOWS 0
+#define MRT_SHADER_WHITTED 1
+#define MRT_SHADER_PATHTRACER 2
+
+/* Samplers (app/Components/Samplers).  The reference draws from std::mt19937 seeded from
+ * /dev/urandom and from process-wide atomic counters, so it is not reproducible; here every draw is
+ * a pure function of (seed, pixel, sample, path node, dimension), identical on the GPU and in the
+ * CPU oracle:
+ *   CONSTANT    value (Constant.cpp:13-15)
+ *   STRATIFIED  frac(sample / spp + r)                 (Stratified.cpp:14-23, counter -> sample)
+ *   HALTON      frac(haltonSequence(sample, p_d) + r)  (HaltonSeq.cpp:14-22, Utils.cpp:36-45)
+ *   RANDOM      hash                                    (MersenneTwister.cpp:9-15)
+ * r is a per-(pixel, node, dimension) rotation from the same hash, p_d the d-th prime. */
+#define MRT_SAMPLER_CONSTANT 0
+#define MRT_SAMPLER_STRATIFIED 1
+#define MRT_SAMPLER_HALTON 2
+#define MRT_SAMPLER_RANDOM 3
+
+#define MRT_LIGHT_POINT 0 /* Components::PointLight (PointLight.cpp:17-26) */
+#define MRT_LIGHT_AREA 1  /* Components::AreaLight  (AreaLight.cpp:22-43)  */
+
+#define MRT_CAMERA_PERSPECTIVE 0 /* Components::Perspective (Perspective.cpp:24-44) */
+
+/* Hit ids: primitive type in the top two bits, index inside that type's array below. */
+#define MRT_PRIM_PLANE 0u
+#define MRT_PRIM_SPHERE 1u
+#define MRT_PRIM_TRIANGLE 2u
+#define MRT_PRIM_LIGHT 3u
+#define MRT_HIT_ID(type, index) ((((uint32_t)(type)) << 30) | ((uint32_t)(index)))
+#define MRT_HIT_TYPE(id) ((uint32_t)(id) >> 30)
+#define MRT_HIT_INDEX(id) ((uint32_t)(id) & 0x3FFFFFFFu)
+#define MRT_HIT_NONE 0xFFFFFFFFu
+
+/* Buffer location flag for the trace/render entry points. */
+#define MRT_MEM_HOST 0u   /* arguments are host pointers; the call copies in and out */
+#define MRT_MEM_DEVICE 1u /* arguments are device pointers on the context's device */
+
+/* ---- plain data types ---------------------------------------------------------------------- */
+/* MobileRT::Material (app/MobileRT/Material.hpp:13-17) */
+typedef struct MrtMaterial {
+    float le[3];  /* emission */
+    float kd[3];  /* diffuse reflection */
+    float ks[3];  /* specular reflection */
+    float kt[3];  /* specular transmission */
+    float ior;    /* refractive index */
+} MrtMaterial;
+
+typedef struct MrtLightDesc {
+    int32_t kind;       /* MRT_LIGHT_POINT or MRT_LIGHT_AREA */
+    float p0[3];        /* point light: position; area light: triangle vertex A */
+    float p1[3];        /* area light: vertex B */
+    float p2[3];        /* area light: vertex C */
+    MrtMaterial radiance;
+} MrtLightDesc;
+
+/* The Scene's vectors as flat host arrays (the CUDA side keeps its own device copies). */
+typedef struct MrtSceneDesc {
+    uint32_t n_triangles;
+    const float *tri_abc;          /* 9 floats per triangle: A, B, C */
+    const float *tri_normals;      /* 9 floats per triangle (nA, nB, nC) or NULL: all three =
+                                      normalize(cross(C - A, B - A)) as in Triangle.cpp:10-17 */
+    const float *tri_colors;       /* 9 floats per triangle or NULL (zero colours) */
+    const int32_t *tri_material;   /* material index per triangle or NULL (-1 = use colours) */
+    uint32_t n_spheres;
+    const float *sphere_center_radius; /* 4 floats per sphere */
+    const int32_t *sphere_material;
+    uint32_t n_planes;
+    const float *plane_point_normal;   /* 6 floats per plane (normal normalised by the library) */
+    const int32_t *plane_material;
+    uint32_t n_materials;
+    const MrtMaterial *materials;
+    uint32_t n_lights;
+    const MrtLightDesc *lights;
+} MrtSceneDesc;
+
+typedef struct MrtAccelOpts {
+    int32_t accelerator;       /* MRT_ACCEL_* */
+    int32_t bvh_mode;          /* MRT_BVH_* */
+    int32_t grid_size;         /* 0 = the reference rule (Shader.cpp:76-105); > 0 forces G for triangles */
+    int32_t grid_index;        /* MRT_GRID_INDEX_* */
+    float camera_position[3];  /* grid bounds include the camera (Shader.cpp:56-62) */
+} MrtAccelOpts;
+
+/* MobileRT::Ray (app/MobileRT/Ray.hpp:14-17); exclude = hit id of the primitive the ray leaves
+ * (the reference compares Ray::primitive_ pointers), MRT_HIT_NONE for camera rays. */
+typedef struct MrtRay {
+    float origin[3];
+    float direction[3];
+    int32_t depth;
+    uint32_t exclude;
+} MrtRay;
+
+typedef struct MrtHit {
+    float t;       /* Intersection::length_; 1e30 (RayLengthMax) on a miss */
+    uint32_t id;   /* MRT_HIT_ID(type, index) or MRT_HIT_NONE */
+} MrtHit;
+
+typedef struct MrtCamera {
+    int32_t kind;         /* MRT_CAMERA_PERSPECTIVE */
+    float position[3];
+    float look_at[3];
+    float up[3];
+    float fov_h_deg;      /* Perspective(position, lookAt, up, hFov, vFov), degrees */
+    float fov_v_deg;
+} MrtCamera;
+
+typedef struct MrtRenderOpts {
+    int32_t shader;         /* MRT_SHADER_* */
+    uint32_t width;         /* Renderer width_ / height_ */
+    uint32_t height;
+    uint32_t spp;           /* samples per pixel (Renderer samplesPixel_) */
+    uint32_t spl;           /* samples per light (Shader samplesLight_) */
+    int32_t pixel_sampler;  /* MRT_SAMPLER_* for the camera-ray jitter */
+    float constant_value;   /* value of a CONSTANT sampler (the reference CLI uses 0.5) */
+    int32_t light_sampler;  /* sampler of AreaLight::getPosition */
+    int32_t rr_sampler;     /* PathTracer Russian-roulette sampler */
+    int32_t depth_min;      /* RayDepthMin (reference 4): Russian roulette only beyond it */
+    int32_t depth_max;      /* RayDepthMax (reference 8): shade() returns black beyond it */
+    uint64_t seed;          /* stream key */
+    uint32_t spp_offset;    /* index of the first sample: a progressive render continues the stream
+                               and the running mean from here */
+    uint32_t reserved;
+} MrtRenderOpts;
+
+typedef struct MrtRenderStats {
+    uint64_t rays_closest;  /* closest-hit rays traced (camera + secondary) */
+    uint64_t rays_shadow;   /* any-hit rays traced */
+    uint64_t paths;         /* camera paths (pixel samples) */
+    float device_ms;        /* device time of the render */
+} MrtRenderStats;
+
+typedef struct MrtContext MrtContext;
+typedef struct MrtScene MrtScene;
+
+/* ---- context -------------------------------------------------------------------------------- */
+int mrt_context_create(int device, MrtContext **out);
+void mrt_context_destroy(MrtContext *ctx);
+const char *mrt_context_error(const MrtContext *ctx);
+int mrt_context_synchronize(MrtContext *ctx);
+/* Stream the context launches on (a cudaStream_t), for callers that order their own work. */
+void *mrt_context_stream(MrtContext *ctx);
+
+/* ---- scene ---------------------------------------------------------------------------------- */
+int mrt_scene_create(MrtContext *ctx, const MrtSceneDesc *desc, MrtScene **out);
+void mrt_scene_destroy(MrtScene *scene);
+int mrt_scene_build(MrtScene *scene, const MrtAccelOpts *opts);
+/* Device bytes held by the scene (geometry + accelerator), for footprint admission. */
+uint64_t mrt_scene_device_bytes(const MrtScene *scene);
+/* Accelerator statistics: nodes (BVH records) or cells (grid), references, grid size. */
+int mrt_scene_accel_info(const MrtScene *scene, uint64_t *nodes, uint64_t *refs, int32_t *grid_size);
+
+/* ---- traversal ------------------------------------------------------------------------------ */
+int mrt_trace_closest(MrtScene *scene, const MrtRay *rays, uint32_t n, MrtHit *hits, uint32_t mem);
+/* occluded[i] = 1 if any plane/sphere/triangle blocks rays[i] within (Epsilon, dist[i]) */
+int mrt_trace_any(MrtScene *scene, const MrtRay *rays, const float *dist, uint32_t n,
+                  uint8_t *occluded, uint32_t mem);
+/* Counting replay of mrt_trace_closest: per-ray node records and triangle records fetched. */
+int mrt_trace_closest_counts(MrtScene *scene, const MrtRay *rays, uint32_t n, uint32_t *node_fetch,
+                             uint32_t *tri_fetch, uint32_t mem);
+
+/* ---- rendering ------------------------------------------------------------------------------ */
+/* One Renderer::renderFrame: for sample = spp_offset .. spp_offset+spp-1 every pixel the reference's
+ * 16x16 block schedule covers gets bitmap = incrementalAvg(rgb, bitmap, sample + 1); other pixels
+ * are left untouched.  stride_bytes / 4 is the row pitch in pixels.  accum (optional, 4 floats per
+ * pixel at width*height) receives the per-pixel sum of the fp32 sample values, in sample order. */
+int mrt_render(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *opts,
+               uint32_t *bitmap, uint32_t stride_bytes, float *accum, uint32_t mem,
+               MrtRenderStats *stats);
+void mrt_render_stop(MrtScene *scene);
+uint32_t mrt_render_progress(const MrtScene *scene);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MRT_CUDA_H */
