@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 render path on the headline workload.
+
+Workload (default): NoShadows, 1920x1080, 1 spp, a 1,000,000-triangle soup (seed 0, centroids
+U[-1,1]^3, edges lognormal(ln 0.005, 0.5), random orientation), one point light, the reference CLI's
+camera, BVH accelerator (built on the device).  One step = one Renderer::renderFrame of that frame
+(mrt_render).  The reference renders rows 0..1071 of a 1080-row image (block height 1080/16 = 67,
+Renderer.cpp:20-21); the rays counted are the rays traced.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun (N > 1) every rank renders its own frame on its own
+GPU (independent frames: weak scaling, no collective on the data path); the timing is the maximum
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH, HEIGHT, N_TRI, SEED = 1920, 1080, 1_000_000, 0
+METRIC = "Mrays/s @1 B200, batched+served vs plain GPU vs host CPU; p50/p99 job latency"
+WORKLOAD = ("config 2: NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point light, "
+            "BVH built on the device")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.path is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic_per_ray():
+    """DRAM bytes per ray of the render kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "render_noshadows_config2.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_ray:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def make_scene():
+    from mobileraytracer_b200 import scenes
+    t0 = time.time()
+    sc = scenes.triangle_soup(N_TRI, SEED, WIDTH, HEIGHT)
+    log(f"scene generated in {time.time() - t0:.1f}s")
+    return sc
+
+
+def cpu_baseline(sc, opts, budget_s: float, threads: int, first: int = 0):
+    """The reference's own CPU renderer (oracle/_ref, compiled from the reference sources with its
+    release optimisation level) on a bounded sample of the frame: every `step`-th pixel."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc as O
+    from mobileraytracer_b200 import capi
+    kind = "reference"
+    try:
+        O.ref(fast=True)
+    except Exception as e:  # the checker library was not built
+        log(f"cpu baseline unavailable: {e}")
+        return None
+    total = WIDTH * HEIGHT
+    # probe: a few rays per thread to estimate the rate
+    probe_step = max(1, total // (threads * 4))
+    _, n, tb, tr = O.ref_render_subset(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, first, probe_step, fast=True)
+    rate = n / max(tr, 1e-6)
+    step = max(1, int(total / max(1.0, rate * budget_s)))
+    _, n, tb2, tr = O.ref_render_subset(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, first + 1, step, fast=True)
+    return {"value": n / tr / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+            "sample": f"every {step}th pixel of the {WIDTH}x{HEIGHT} frame ({n} camera rays), reference BVH "
+                      f"(build {tb:.2f}s), {threads} threads", "rays": n, "seconds": tr, "build_seconds": tb}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU implementation of the path on the host cores."""
+    ws, rank, local = dist_info()
+    if rank != 0:
+        return
+    from mobileraytracer_b200 import capi
+    sc = make_scene()
+    opts = capi.render_opts(shader=capi.MRT_SHADER_NOSHADOWS, width=WIDTH, height=HEIGHT, spp=1, spl=1)
+    threads = os.cpu_count() or 1
+    per_step = max(1.5, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc as O
+    try:
+        O.ref(fast=True)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU library not built: {e}"}))
+        return
+    total = WIDTH * HEIGHT
+    _, n, tb, tr = O.ref_render_subset(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, 0, max(1, total // (threads * 4)), fast=True)
+    rate = n / max(tr, 1e-6)
+    step = max(1, int(total / max(1.0, rate * per_step)))
+    for w in range(args.warmup):
+        O.ref_render_subset(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, w + 1, step, fast=True)
+    rays, secs = 0, 0.0
+    for k in range(args.steps):
+        _, n, _, tr = O.ref_render_subset(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, args.warmup + 1 + k,
+                                          step, fast=True)
+        rays += n
+        secs += tr
+    value = rays / secs / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_per_step": f"every {step}th pixel", "accelerator": "reference BVH"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                         "sample": f"every {step}th pixel of the {WIDTH}x{HEIGHT} frame per step, reference BVH "
+                                   f"(build {tb:.2f}s), {threads} threads"},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import mobileraytracer_b200 as m
+    from mobileraytracer_b200 import camera as mcam
+    from mobileraytracer_b200 import capi
+
+    sc = make_scene()
+    ctx = m.Context(local)
+    t0 = time.time()
+    scene = m.Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
+    build_s = time.time() - t0
+    opts = capi.render_opts(shader=capi.MRT_SHADER_NOSHADOWS, width=WIDTH, height=HEIGHT, spp=1, spl=1)
+    bitmap = torch.zeros(WIDTH * HEIGHT, dtype=torch.int32, device=f"cuda:{local}")
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)   # evicts L2 (126 MB) before every step; not inside the timed events
+        _, _, st = scene.render(sc.camera, opts, bitmap=bitmap)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    dev_ms, rays = 0.0, 0
+    wall0 = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            st = step()
+            dev_ms += st.device_ms
+            rays += st.rays_closest
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    if ws > 1:
+        t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        torch.distributed.barrier()
+    rays_per_step = rays // args.steps
+    value = rays_per_step * args.steps * ws / (dev_ms / 1e3) / 1e6
+    ms_per_step = dev_ms / args.steps
+
+    # end to end through the C ABI with host buffers: pinned bitmap in, render, bitmap out
+    host_bm = torch.zeros(WIDTH * HEIGHT, dtype=torch.int32).pin_memory()
+    host_np = host_bm.numpy()
+    scene.render(sc.camera, opts, bitmap=host_np)
+    e2e_t = 0.0
+    e2e_n = max(1, min(args.e2e_steps, args.steps))
+    for _ in range(e2e_n):
+        t1 = time.perf_counter()
+        scene.render(sc.camera, opts, bitmap=host_np)
+        e2e_t += time.perf_counter() - t1
+    e2e_value = rays_per_step * e2e_n * ws / e2e_t / 1e6
+    bm_bytes = WIDTH * HEIGHT * 4
+
+    # roofline: algorithmic bytes per launch from the counting replay over the same camera rays
+    rays_np = mcam.primary_rays(sc.camera, WIDTH, HEIGHT, pixels=np.arange(WIDTH * 16 * (HEIGHT // 16)))
+    nodes, tris = scene.trace_counts(rays_np)
+    hits = scene.trace_closest(rays_np)
+    n_hit = int(np.sum((hits["id"] >> 30) == capi.MRT_PRIM_TRIANGLE))
+    alg_bytes = 8 * len(rays_np) + 32 * int(nodes.sum(dtype=np.int64)) + 48 * int(tris.sum(dtype=np.int64)) + 76 * n_hit
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    tpr = profiled_traffic_per_ray()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": (tpr * len(rays_np)) if tpr else None,
+            "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": alg_bytes / len(rays_np),
+            "node_records_per_ray": float(nodes.mean()), "tri_records_per_ray": float(tris.mean()),
+            "kernel": "k_render_noshadows<BVH,FAST>"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sc, opts, args.cpu_budget, os.cpu_count() or 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": rays_per_step, "rows_rendered": 16 * (HEIGHT // 16),
+                   "l2": "flushed before every step (512 MiB write outside the timed events)",
+                   "bvh_build_seconds": build_s, "wall_seconds_timed_loop": wall, "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": bm_bytes + 64 + 100,
+                "d2h_bytes_per_step": bm_bytes},
+        "gpu_launches": args.steps,
+        "roofline": roof,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,2 +1,182 @@
-"""B200 render path for MobileRT (MobileRayTracer): CUDA kernels behind the C ABI of
-include/mrt_cuda.h, with Python bindings for tests and benchmarks."""
+"""B200 render path for MobileRT (MobileRayTracer).
+
+The work happens in CUDA kernels behind the C ABI of include/mrt_cuda.h (libmrt_cuda.so, built by
+``python -m mobileraytracer_b200.build``).  This module is a thin Python binding of that ABI for
+tests and benchmarks; it has no compute of its own and no CPU fallback: every call goes to the
+device and raises MrtError when the library or the GPU is unavailable.
+
+    ctx = Context(0)
+    scn = Scene(ctx, scenes.triangle_soup(1_000_000))
+    scn.build(capi.MRT_ACCEL_BVH)
+    bitmap, accum, stats = scn.render(camera, capi.render_opts(width=1920, height=1080))
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+
+__all__ = ["Context", "Scene", "MrtError", "capi"]
+
+RAY_DTYPE = np.dtype([("origin", np.float32, 3), ("direction", np.float32, 3), ("depth", np.int32),
+                      ("exclude", np.uint32)])
+HIT_DTYPE = np.dtype([("t", np.float32), ("id", np.uint32)])
+
+
+class MrtError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{capi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+def _ptr(x):
+    """(pointer, mem flag) for a numpy array (host) or a CUDA torch tensor (device)."""
+    if _is_torch_cuda(x):
+        return ctypes.c_void_p(x.data_ptr()), capi.MRT_MEM_DEVICE
+    a = np.ascontiguousarray(x)
+    return ctypes.c_void_p(a.ctypes.data), capi.MRT_MEM_HOST
+
+
+class Context:
+    """One CUDA device and stream (MrtContext)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = capi.load()
+        h = ctypes.c_void_p()
+        st = self.lib.mrt_context_create(device, ctypes.byref(h))
+        if st != capi.MRT_OK:
+            raise MrtError(st, f"mrt_context_create(device={device}) failed")
+        self.h = h
+        self.device = device
+
+    def check(self, st: int, what: str):
+        if st != capi.MRT_OK:
+            raise MrtError(st, f"{what}: {self.lib.mrt_context_error(self.h).decode(errors='replace')}")
+
+    def synchronize(self):
+        self.check(self.lib.mrt_context_synchronize(self.h), "synchronize")
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.mrt_context_stream(self.h) or 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mrt_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """A device-resident scene (MrtScene) with its accelerator."""
+
+    def __init__(self, ctx: Context, scene):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.host = scene
+        self._desc = scene.desc()
+        h = ctypes.c_void_p()
+        ctx.check(self.lib.mrt_scene_create(ctx.h, ctypes.byref(self._desc), ctypes.byref(h)), "mrt_scene_create")
+        self.h = h
+
+    def build(self, accelerator: int = capi.MRT_ACCEL_BVH, bvh_mode: int = capi.MRT_BVH_FAST, grid_size: int = 0,
+              grid_index: int = capi.MRT_GRID_INDEX_REFERENCE, camera_position=None):
+        o = capi.MrtAccelOpts()
+        o.accelerator, o.bvh_mode, o.grid_size, o.grid_index = accelerator, bvh_mode, grid_size, grid_index
+        if camera_position is None:
+            camera_position = list(self.host.camera.position) if self.host.camera is not None else [0.0, 0.0, 0.0]
+        o.camera_position[:] = camera_position
+        self.ctx.check(self.lib.mrt_scene_build(self.h, ctypes.byref(o)), "mrt_scene_build")
+        return self
+
+    def device_bytes(self) -> int:
+        return int(self.lib.mrt_scene_device_bytes(self.h))
+
+    def accel_info(self):
+        n, r, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
+        self.lib.mrt_scene_accel_info(self.h, ctypes.byref(n), ctypes.byref(r), ctypes.byref(g))
+        return {"nodes": n.value, "refs": r.value, "grid_size": g.value}
+
+    def trace_closest(self, rays, hits=None):
+        n = len(rays)
+        if hits is None:
+            if _is_torch_cuda(rays):
+                import torch
+                hits = torch.empty((n, 2), dtype=torch.int32, device=rays.device)
+            else:
+                hits = np.zeros(n, HIT_DTYPE)
+        rp, mem = _ptr(rays)
+        hp, mem2 = _ptr(hits)
+        assert mem == mem2, "rays and hits must both be host or both be device buffers"
+        self.ctx.check(self.lib.mrt_trace_closest(self.h, rp, n, hp, mem), "mrt_trace_closest")
+        return hits
+
+    def trace_any(self, rays, dist, occluded=None):
+        n = len(rays)
+        if occluded is None:
+            if _is_torch_cuda(rays):
+                import torch
+                occluded = torch.empty(n, dtype=torch.uint8, device=rays.device)
+            else:
+                occluded = np.zeros(n, np.uint8)
+        rp, mem = _ptr(rays)
+        dp, _ = _ptr(dist if _is_torch_cuda(dist) else np.ascontiguousarray(dist, np.float32))
+        op, _ = _ptr(occluded)
+        self.ctx.check(self.lib.mrt_trace_any(self.h, rp, dp, n, op, mem), "mrt_trace_any")
+        return occluded
+
+    def trace_counts(self, rays):
+        n = len(rays)
+        nodes = np.zeros(n, np.uint32)
+        tris = np.zeros(n, np.uint32)
+        rp, mem = _ptr(rays)
+        self.ctx.check(self.lib.mrt_trace_closest_counts(self.h, rp, n, ctypes.c_void_p(nodes.ctypes.data),
+                                                         ctypes.c_void_p(tris.ctypes.data), capi.MRT_MEM_HOST),
+                       "mrt_trace_closest_counts")
+        return nodes, tris
+
+    def render(self, camera, opts, bitmap=None, accum=None, stride_bytes: int | None = None):
+        """One Renderer::renderFrame.  numpy buffers -> host path (copies inside the call);
+        CUDA tensors -> device path.  Returns (bitmap, accum, MrtRenderStats)."""
+        w, h = opts.width, opts.height
+        if bitmap is None:
+            bitmap = np.zeros((h, w), np.uint32)
+        if stride_bytes is None:
+            stride_bytes = w * 4
+        bp, mem = _ptr(bitmap)
+        ap = None
+        if accum is not None:
+            ap, mem2 = _ptr(accum)
+            assert mem == mem2
+        stats = capi.MrtRenderStats()
+        self.ctx.check(self.lib.mrt_render(self.h, ctypes.byref(camera), ctypes.byref(opts), bp, stride_bytes, ap, mem,
+                                           ctypes.byref(stats)), "mrt_render")
+        return bitmap, accum, stats
+
+    def stop(self):
+        self.lib.mrt_render_stop(self.h)
+
+    def progress(self) -> int:
+        return int(self.lib.mrt_render_progress(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mrt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

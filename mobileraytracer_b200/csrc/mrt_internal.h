@@ -1,0 +1,83 @@
+// mrt_internal.h - host-side state behind the C ABI (not part of the public interface).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/mrt_cuda.h"
+#include "mrt_device.cuh"
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct MrtContext {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    int sm_count = 148;
+    int32_t *d_error = nullptr;         // device error flag (MRT_ERR_LIMIT from kernels)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // reusable scratch for host-pointer calls
+    DevBuf scratch[4];
+};
+
+struct RefBvhHost {
+    std::vector<mrt::RefNode> nodes;
+};
+
+struct MrtScene {
+    MrtContext *ctx = nullptr;
+    mrt::DevScene dev{};
+    // geometry
+    uint32_t n_tri = 0, n_sph = 0, n_pln = 0, n_light = 0, n_mat = 0;
+    DevBuf tri_a, tri_ab, tri_ac, tri_n, tri_c, tri_mat, sph, sph_mat, pln_n, pln_p, pln_mat, lights, mats;
+    // accelerators
+    bool built = false;
+    MrtAccelOpts opts{};
+    DevBuf fnodes, ftris;
+    uint64_t fnode_count = 0;
+    DevBuf rnodes[3];
+    uint64_t rnode_count[3] = {0, 0, 0};
+    DevBuf grid_start[3], grid_refs[3];
+    uint64_t grid_refs_count[3] = {0, 0, 0};
+    // host copies needed by the reference-tree build and the grid bounds
+    std::vector<float> h_abc;           // 9 floats per triangle
+    std::vector<float> h_sph;           // 4 per sphere
+    std::vector<float> h_pln;           // 6 per plane (point, normalised normal)
+    // render state
+    std::atomic<uint32_t> progress{0};
+    std::atomic<int> stop{0};
+    DevBuf work[8];                     // render scratch (wavefront pools, per-pixel buffers)
+};
+
+namespace mrt_host {
+
+bool set_error(MrtContext *ctx, const char *fmt, ...);
+int cuda_status(MrtContext *ctx, cudaError_t e, const char *what);
+int dev_alloc(MrtContext *ctx, DevBuf &b, size_t bytes);
+void dev_free(DevBuf &b);
+int ensure(MrtContext *ctx, DevBuf &b, size_t bytes);   // grow-only scratch
+int check_kernel_error(MrtContext *ctx);                // reads and clears the device error flag
+
+// builds (mrt_bvh.cu, mrt_grid.cu)
+int build_fast_bvh(MrtScene *s);
+int build_reference_bvh(MrtScene *s);
+int build_grids(MrtScene *s, const float *camera_position, int grid_size, int grid_index);
+
+// kernels (mrt_kernels.cu)
+int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits);
+int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uint32_t n, uint8_t *d_occ);
+int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris);
+int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
+           float *d_accum, MrtRenderStats *stats);
+
+mrt::DevCamera make_camera(const MrtCamera &c);
+
+}  // namespace mrt_host

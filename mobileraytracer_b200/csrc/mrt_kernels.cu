@@ -1,0 +1,107 @@
+// mrt_kernels.cu - batch traversal kernels behind mrt_trace_closest / mrt_trace_any /
+// mrt_trace_closest_counts.  One thread per ray; rays are 32-byte MrtRay records read as two
+// 128-bit loads.
+#include "mrt_internal.h"
+#include "mrt_trace.cuh"
+
+using namespace mrt;
+using namespace mrt_host;
+
+namespace {
+
+__device__ __forceinline__ Ray load_ray(const MrtRay *rays, uint32_t i) {
+    const float4 *p = reinterpret_cast<const float4 *>(rays) + 2 * (size_t)i;
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    Ray r;
+    r.o = V3{a.x, a.y, a.z};
+    r.d = V3{a.w, b.x, b.y};
+    r.depth = __float_as_int(b.z);
+    r.exclude = __float_as_uint(b.w);
+    return r;
+}
+
+template <int ACCEL, int MODE>
+__global__ void __launch_bounds__(128) k_trace_closest(DevScene s, const MrtRay *rays, uint32_t n, MrtHit *hits) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Ray r = load_ray(rays, i);
+        float len;
+        uint32_t id;
+        const bool hit = scene_closest<ACCEL, MODE>(s, r, len, id);
+        MrtHit h;
+        h.t = hit ? len : kRayLengthMax;
+        h.id = hit ? id : MRT_HIT_NONE;
+        reinterpret_cast<uint2 *>(hits)[i] = make_uint2(__float_as_uint(h.t), h.id);
+    }
+}
+
+template <int ACCEL, int MODE>
+__global__ void __launch_bounds__(128) k_trace_any(DevScene s, const MrtRay *rays, const float *dist, uint32_t n,
+                                                   uint8_t *occ) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Ray r = load_ray(rays, i);
+        occ[i] = scene_occ<ACCEL, MODE>(s, r, dist[i]) ? 1 : 0;
+    }
+}
+
+// counting replay of the FAST traversal: per ray, node records and triangle records fetched
+__global__ void __launch_bounds__(128) k_trace_counts(DevScene s, const MrtRay *rays, uint32_t n, uint32_t *nodes,
+                                                      uint32_t *tris) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Ray r = load_ray(rays, i);
+        float len = kRayLengthMax;
+        uint32_t id = MRT_HIT_NONE;
+        naive_trace<kPlane>(s, r, len, id);
+        naive_trace<kSphere>(s, r, len, id);
+        FastCounts c{0, 0};
+        fast_trace<true>(s, r, len, id, &c);
+        nodes[i] = c.nodes;
+        tris[i] = c.tris;
+    }
+}
+
+template <int ACCEL, int MODE>
+void launch_closest(const DevScene &s, const MrtRay *rays, uint32_t n, MrtHit *hits, int grid, cudaStream_t q) {
+    k_trace_closest<ACCEL, MODE><<<grid, 128, 0, q>>>(s, rays, n, hits);
+}
+template <int ACCEL, int MODE>
+void launch_any(const DevScene &s, const MrtRay *rays, const float *dist, uint32_t n, uint8_t *occ, int grid, cudaStream_t q) {
+    k_trace_any<ACCEL, MODE><<<grid, 128, 0, q>>>(s, rays, dist, n, occ);
+}
+
+#define MRT_DISPATCH(fn, accel, mode, ...)                                                                 \
+    do {                                                                                                    \
+        if ((accel) == MRT_ACCEL_NAIVE) fn<MRT_ACCEL_NAIVE, MRT_BVH_FAST>(__VA_ARGS__);                     \
+        else if ((accel) == MRT_ACCEL_REGULAR_GRID) fn<MRT_ACCEL_REGULAR_GRID, MRT_BVH_FAST>(__VA_ARGS__);  \
+        else if ((mode) == MRT_BVH_REFERENCE) fn<MRT_ACCEL_BVH, MRT_BVH_REFERENCE>(__VA_ARGS__);            \
+        else fn<MRT_ACCEL_BVH, MRT_BVH_FAST>(__VA_ARGS__);                                                  \
+    } while (0)
+
+int grid_for(const MrtContext *ctx, uint32_t n) {
+    const uint32_t want = (n + 127) / 128;
+    const uint32_t cap = (uint32_t)ctx->sm_count * 16u;
+    return (int)(want < cap ? (want ? want : 1) : cap);
+}
+
+}  // namespace
+
+namespace mrt_host {
+
+int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits) {
+    MrtContext *ctx = s->ctx;
+    MRT_DISPATCH(launch_closest, s->opts.accelerator, s->opts.bvh_mode, s->dev, d_rays, n, d_hits, grid_for(ctx, n), ctx->stream);
+    return cuda_status(ctx, cudaGetLastError(), "k_trace_closest");
+}
+
+int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uint32_t n, uint8_t *d_occ) {
+    MrtContext *ctx = s->ctx;
+    MRT_DISPATCH(launch_any, s->opts.accelerator, s->opts.bvh_mode, s->dev, d_rays, d_dist, n, d_occ, grid_for(ctx, n), ctx->stream);
+    return cuda_status(ctx, cudaGetLastError(), "k_trace_any");
+}
+
+int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris) {
+    MrtContext *ctx = s->ctx;
+    k_trace_counts<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(s->dev, d_rays, n, d_nodes, d_tris);
+    return cuda_status(ctx, cudaGetLastError(), "k_trace_counts");
+}
+
+}  // namespace mrt_host

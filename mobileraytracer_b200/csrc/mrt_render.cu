@@ -1,0 +1,803 @@
+// mrt_render.cu - Renderer::renderFrame on the device (Renderer.cpp:31-116).
+//
+// Pixels: the reference renders 16x16 blocks handed out in a shuffled Halton order
+// (Camera.cpp:13-37, Renderer.cpp:79-93); each visited pixel gets, per sample pass,
+// bitmap = incrementalAvg(rgb, bitmap, sample + 1).  The host enumerates the visited pixels with the
+// reference's block arithmetic; when they form the rectangle [0,W) x [0,16*(H/16)) with no pixel
+// visited twice (the usual case) the kernels map threads to pixels directly, otherwise they walk an
+// explicit task list in block order, one round per repeated visit.
+//
+// NoShadows (NoShadows.cpp:19-65) has no secondary rays: one fused kernel does camera ray, closest
+// hit, shading and the running mean per pixel.
+//
+// Whitted and PathTracer (Whitted.cpp:17-107, PathTracer.cpp:25-164) recurse.  Here they run as a
+// wavefront over a wave of camera paths: per bounce level an extend kernel (closest hit), a shade
+// kernel that writes one node record per ray and appends shadow rays and continuation rays to
+// queues compacted with warp ballots, and an any-hit kernel for the shadow queue.  After the last
+// level the nodes are resolved bottom-up, level by level, combining each node's own terms with its
+// children's results in the reference's order of operations, so the per-sample value equals the
+// recursive one bit for bit.  Per-sample values are then folded into the bitmap in sample order.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "mrt_internal.h"
+#include "mrt_trace.cuh"
+
+using namespace mrt;
+using namespace mrt_host;
+
+namespace {
+
+struct Task {
+    uint32_t x, y, index;
+};
+
+struct RenderParams {
+    DevCamera cam;
+    uint32_t width, height, spp, spl, stride_px;
+    int32_t pixel_sampler, light_sampler, rr_sampler, shader;
+    float constant_value;
+    int32_t depth_min, depth_max;
+    uint64_t seed;
+    uint32_t spp_offset;
+    uint32_t strata;       // spp of the whole render (Stratified sampler strata)
+    uint32_t task_base;    // first task of the current round (wavefront)
+    // tasks: implicit rectangle (tasks == nullptr: x = t % width, y = t / width) or explicit list
+    const Task *tasks;
+    uint32_t n_tasks;
+    uint32_t *bitmap;
+    float4 *accum;
+    float inv_w, inv_h, pw, ph;
+};
+
+__device__ __forceinline__ Task task_of(const RenderParams &p, uint32_t t) {
+    if (p.tasks) return p.tasks[t];
+    Task k;
+    k.x = t % p.width;
+    k.y = t / p.width;
+    k.index = k.y * p.stride_px + k.x;
+    return k;
+}
+
+__device__ __forceinline__ Ray primary_ray(const RenderParams &p, const Task &k, const Stream &st) {
+    const float u = (float)k.x * p.inv_w, v = (float)k.y * p.inv_h;   // Renderer.cpp:95-99
+    const float r1 = draw(st, p.pixel_sampler, 0u, 0u);
+    const float r2 = draw(st, p.pixel_sampler, 0u, 1u);
+    return camera_ray(p.cam, u, v, (r1 - 0.5f) * 2.0f * p.pw, (r2 - 0.5f) * 2.0f * p.ph);
+}
+
+// Shader::getLight (Shader.cpp:225-236) and Light::getPosition (PointLight.cpp:17-19,
+// AreaLight.cpp:22-31) for light sample j of a node
+__device__ __forceinline__ const DevLight &pick_light(const DevScene &s, const Stream &st, uint32_t node, uint32_t j) {
+    const float u = key_float(st.base, node, kDimLight + 3u * j);
+    const uint32_t k = (uint32_t)floorf(u * (float)s.n_light * 0.99999f);
+    return s.lights[k];
+}
+__device__ __forceinline__ V3 light_position(const DevLight &l, const Stream &st, int kind, uint32_t node, uint32_t j) {
+    if (l.kind != MRT_LIGHT_AREA) return l.pos;
+    float R = draw(st, kind, node, kDimLight + 3u * j + 1u);
+    float S = draw(st, kind, node, kDimLight + 3u * j + 2u);
+    if (R + S >= 1.0f) { R = 1.0f - R; S = 1.0f - S; }
+    return (l.a + l.ab * R) + l.ac * S;
+}
+
+__device__ __forceinline__ bool material_of(const DevScene &s, const Isect &it, DevMaterial &m) {
+    if (it.light >= 0) { m = s.lights[it.light].radiance; return true; }
+    if (it.mat >= 0) { m = s.mats[it.mat]; return true; }
+    return false;
+}
+
+// NoShadows::shade, NoShadows.cpp:19-65
+__device__ __forceinline__ V3 shade_noshadows(const DevScene &s, const RenderParams &p, const Stream &st, const Isect &it,
+                                              uint32_t node) {
+    V3 rgb{0.0f, 0.0f, 0.0f};
+    V3 kd;
+    DevMaterial m;
+    if (material_of(s, it, m)) {
+        if (any_pos(m.le)) return m.le;
+        kd = m.kd;
+    } else {
+        kd = it.color;
+    }
+    if (any_pos(kd) && s.n_light > 0) {
+        for (uint32_t j = 0; j < p.spl; ++j) {
+            const DevLight &l = pick_light(s, st, node, j);
+            const V3 lp = light_position(l, st, p.light_sampler, node, j);
+            const V3 vtl = normalize(lp - it.point);
+            const float c = dot(it.normal, vtl);
+            if (c > 0.0f) rgb = rgb + l.radiance.le * c;
+        }
+        rgb = rgb * kd;
+        rgb = rgb / (float)p.spl;
+    }
+    return rgb + kd * 0.1f;
+}
+
+template <int ACCEL, int MODE>
+__global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderParams p, uint32_t round_first,
+                                                          uint32_t round_count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < round_count; i += gridDim.x * blockDim.x) {
+        const uint32_t t = round_first + i;
+        const Task k = task_of(p, t);
+        const uint32_t pixel = k.y * p.width + k.x;
+        uint32_t bm = p.bitmap[k.index];
+        float4 acc = p.accum ? p.accum[pixel] : make_float4(0, 0, 0, 0);
+        for (uint32_t si = 0; si < p.spp; ++si) {
+            const uint32_t sample = p.spp_offset + si;
+            const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+            const Ray r = primary_ray(p, k, st);
+            V3 rgb{0.0f, 0.0f, 0.0f};
+            float len;
+            uint32_t id;
+            if (scene_closest<ACCEL, MODE>(s, r, len, id)) {
+                Isect it;
+                if (make_isect(s, r, id, it)) rgb = shade_noshadows(s, p, st, it, 1u);
+            }
+            bm = incremental_avg(rgb, bm, sample + 1u);
+            acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
+        }
+        p.bitmap[k.index] = bm;
+        if (p.accum) p.accum[pixel] = acc;
+    }
+}
+
+// ============================== wavefront ====================================================
+enum NodeKind : uint32_t { kMiss = 0, kEmit = 1, kCut = 2, kShaded = 3 };
+enum NodeFlag : uint32_t { kHasIndirect = 4, kRRScaled = 8, kKdPos = 16, kKsPos = 32, kKtPos = 64 };
+
+struct RayRec {          // 48 bytes
+    float ox, oy, oz, dx, dy, dz;
+    int32_t depth;
+    uint32_t exclude;
+    uint32_t root;       // wave-local root index
+    uint32_t parent;     // node index of the parent (0xFFFFFFFF for camera rays)
+    uint32_t slot;       // 0 indirect, 1 specular, 2 transmission
+    uint32_t code;       // path-tree code keying the stream (root 1, child code*4 + slot + 1)
+};
+
+struct NodeRec {         // 128 bytes
+    uint32_t flags;      // kind | NodeFlag
+    uint32_t occluded;   // bit j: shadow ray of light sample j was blocked
+    float hit_t;
+    uint32_t hit_id;
+    V3 kd, ks, kt;       // 36
+    V3 point, normal;    // 24 (or rgb of an emitter in `point`)
+    V3 child[3];         // 36
+    uint32_t child_flag; // bit s: child s reported a light hit
+    uint32_t pad[3];
+};
+
+struct ShadowRec {       // 40 bytes
+    float ox, oy, oz, dx, dy, dz, dist;
+    uint32_t node;
+    uint32_t j;
+    uint32_t exclude;
+};
+
+struct Level {
+    uint32_t start;
+    uint32_t count;
+    uint32_t shadow_count;
+    uint32_t pad;
+};
+
+struct WaveState {
+    RayRec *rays;
+    NodeRec *nodes;
+    ShadowRec *shadows;
+    Level *levels;           // [max_levels + 1]
+    float4 *root_rgb;        // per wave root: rgb, flag
+    uint32_t ray_cap;
+    uint32_t shadow_cap;
+    uint32_t root_first;     // global index of the wave's first root
+    uint32_t n_roots;
+    unsigned long long *counters;   // [0] closest rays, [1] shadow rays
+};
+
+__device__ __forceinline__ uint32_t warp_alloc(uint32_t want, uint32_t *counter) {
+    // warp-aggregated allocation: inclusive scan of `want` across the warp, one atomic per warp.
+    // Every lane of the warp calls this (the shade loop runs whole warps).
+    __syncwarp();
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = want;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    uint32_t base = 0;
+    if (lane == 31 && incl > 0) base = atomicAdd(counter, incl);
+    base = __shfl_sync(0xFFFFFFFFu, base, 31);
+    return base + incl - want;
+}
+
+__device__ __forceinline__ void root_task(const RenderParams &p, const WaveState &w, uint32_t root, Task &k,
+                                          uint32_t &pixel, uint32_t &sample) {
+    const uint32_t g = w.root_first + root;
+    const uint32_t t = p.task_base + g / p.spp, si = g % p.spp;
+    k = task_of(p, t);
+    pixel = k.y * p.width + k.x;
+    sample = p.spp_offset + si;
+}
+
+__global__ void k_wave_raygen(RenderParams p, WaveState w) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n_roots; i += gridDim.x * blockDim.x) {
+        Task k;
+        uint32_t pixel, sample;
+        root_task(p, w, i, k, pixel, sample);
+        const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+        const Ray r = primary_ray(p, k, st);
+        RayRec rr;
+        rr.ox = r.o.x; rr.oy = r.o.y; rr.oz = r.o.z;
+        rr.dx = r.d.x; rr.dy = r.d.y; rr.dz = r.d.z;
+        rr.depth = 1;
+        rr.exclude = MRT_HIT_NONE;
+        rr.root = i;
+        rr.parent = 0xFFFFFFFFu;
+        rr.slot = 0;
+        rr.code = 1u;
+        w.rays[i] = rr;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.levels[0].start = 0;
+        w.levels[0].count = w.n_roots;
+        w.levels[0].shadow_count = 0;
+    }
+}
+
+__device__ __forceinline__ Ray ray_of(const RayRec &r) {
+    Ray x;
+    x.o = V3{r.ox, r.oy, r.oz};
+    x.d = V3{r.dx, r.dy, r.dz};
+    x.depth = r.depth;
+    x.exclude = r.exclude;
+    return x;
+}
+
+__device__ __forceinline__ Level clamp_level(const WaveState &w, Level L) {
+    // a level never reaches past the ray pool (overflowing children were dropped with MRT_ERR_LIMIT)
+    L.start = min(L.start, w.ray_cap);
+    L.count = min(L.count, w.ray_cap - L.start);
+    return L;
+}
+
+template <int ACCEL, int MODE>
+__global__ void __launch_bounds__(128) k_wave_extend(DevScene s, WaveState w, int level) {
+    const Level L = clamp_level(w, w.levels[level]);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
+        const uint32_t idx = L.start + i;
+        const Ray r = ray_of(w.rays[idx]);
+        float len;
+        uint32_t id;
+        const bool hit = scene_closest<ACCEL, MODE>(s, r, len, id);
+        w.nodes[idx].hit_t = len;
+        w.nodes[idx].hit_id = hit ? id : MRT_HIT_NONE;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
+}
+
+__global__ void __launch_bounds__(128) k_wave_shade(DevScene s, RenderParams p, WaveState w, int level) {
+    const Level L = clamp_level(w, w.levels[level]);
+    Level *next = &w.levels[level + 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) next->start = L.start + L.count;
+    const uint32_t next_start = L.start + L.count;
+    const uint32_t n_iter = (L.count + blockDim.x - 1) / blockDim.x;   // whole warps iterate together
+    for (uint32_t it_ = blockIdx.x; it_ < n_iter; it_ += gridDim.x) {
+        const uint32_t i = it_ * blockDim.x + threadIdx.x;
+        const bool active = i < L.count;
+        const uint32_t idx = L.start + (active ? i : 0);
+        uint32_t n_child = 0, n_shadow = 0;
+        Ray child[3];
+        uint32_t child_slot[3];
+        NodeRec nd;
+        RayRec rr;
+        Isect isect;
+        Stream st;
+        bool shaded = false;
+        if (active) {
+            rr = w.rays[idx];
+            const Ray r = ray_of(rr);
+            nd.flags = kMiss;
+            nd.occluded = 0;
+            nd.child_flag = 0;
+            nd.child[0] = nd.child[1] = nd.child[2] = V3{0, 0, 0};
+            nd.kd = nd.ks = nd.kt = V3{0, 0, 0};
+            nd.point = nd.normal = V3{0, 0, 0};
+            const uint32_t hit_id = w.nodes[idx].hit_id;
+            nd.hit_id = hit_id;
+            nd.hit_t = w.nodes[idx].hit_t;
+            Task k;
+            uint32_t pixel, sample;
+            root_task(p, w, rr.root, k, pixel, sample);
+            st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+            if (hit_id != MRT_HIT_NONE && make_isect(s, r, hit_id, isect)) {
+                if (r.depth > p.depth_max) {
+                    nd.flags = kCut;   // Whitted.cpp:20-22, PathTracer.cpp:28-31
+                } else {
+                    DevMaterial m;
+                    V3 kd, ks{0, 0, 0}, kt{0, 0, 0};
+                    float ior = 1.0f;
+                    bool emitted = false;
+                    if (material_of(s, isect, m)) {
+                        if (any_pos(m.le)) { nd.flags = kEmit; nd.point = m.le; emitted = true; }
+                        kd = m.kd; ks = m.ks; kt = m.kt; ior = m.ior;
+                    } else {
+                        kd = isect.color;
+                    }
+                    if (!emitted) {
+                        shaded = true;
+                        nd.flags = kShaded;
+                        nd.kd = kd; nd.ks = ks; nd.kt = kt;
+                        nd.point = isect.point;
+                        nd.normal = isect.normal;
+                        const bool kd_pos = any_pos(kd), ks_pos = any_pos(ks), kt_pos = any_pos(kt);
+                        if (kd_pos) nd.flags |= kKdPos;
+                        if (ks_pos) nd.flags |= kKsPos;
+                        if (kt_pos) nd.flags |= kKtPos;
+                        if (kd_pos && s.n_light > 0) {
+                            for (uint32_t j = 0; j < p.spl; ++j) {
+                                const DevLight &l = pick_light(s, st, rr.code, j);
+                                const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
+                                const V3 vtl = normalize(lp - isect.point);
+                                if (dot(isect.normal, vtl) > 0.0f) ++n_shadow;
+                            }
+                        }
+                        if (p.shader == MRT_SHADER_PATHTRACER && kd_pos) {
+                            bool go = r.depth <= p.depth_min;   // PathTracer.cpp:106-107
+                            if (!go) go = draw(st, p.rr_sampler, rr.code, kDimRR) > 0.5f;
+                            if (go) {
+                                nd.flags |= kHasIndirect;
+                                if (r.depth > p.depth_min) nd.flags |= kRRScaled;
+                                Ray c;
+                                c.o = isect.point;
+                                c.d = hemisphere(isect.normal, key_float(st.base, rr.code, kDimHemi),
+                                                 key_float(st.base, rr.code, kDimHemi + 1u));
+                                c.depth = r.depth + 1;
+                                c.exclude = isect.prim;
+                                child[n_child] = c;
+                                child_slot[n_child++] = 0;
+                            }
+                        }
+                        if (ks_pos) {
+                            Ray c;
+                            c.o = isect.point;
+                            c.d = reflect(r.d, isect.normal);
+                            c.depth = r.depth + 1;
+                            c.exclude = isect.prim;
+                            child[n_child] = c;
+                            child_slot[n_child++] = 1;
+                        }
+                        if (kt_pos) {
+                            Ray c;
+                            c.o = isect.point;
+                            c.d = refract(r.d, isect.normal, 1.0f / ior);
+                            c.depth = r.depth + 1;
+                            c.exclude = isect.prim;
+                            child[n_child] = c;
+                            child_slot[n_child++] = 2;
+                        }
+                    }
+                }
+            }
+            w.nodes[idx] = nd;
+        }
+        // queue compaction: one atomic per warp for children, one for shadow rays
+        const uint32_t cbase = warp_alloc(n_child, &next->count);
+        const uint32_t sbase = warp_alloc(n_shadow, &w.levels[level].shadow_count);
+        if (!active) continue;
+        for (uint32_t c = 0; c < n_child; ++c) {
+            const uint32_t pos = next_start + cbase + c;
+            if (pos >= w.ray_cap) { raise_error(s, MRT_ERR_LIMIT); break; }
+            RayRec o;
+            o.ox = child[c].o.x; o.oy = child[c].o.y; o.oz = child[c].o.z;
+            o.dx = child[c].d.x; o.dy = child[c].d.y; o.dz = child[c].d.z;
+            o.depth = child[c].depth;
+            o.exclude = child[c].exclude;
+            o.root = rr.root;
+            o.parent = idx;
+            o.slot = child_slot[c];
+            o.code = rr.code * 4u + child_slot[c] + 1u;
+            w.rays[pos] = o;
+        }
+        if (shaded && n_shadow) {
+            uint32_t q = 0;
+            for (uint32_t j = 0; j < p.spl; ++j) {
+                const DevLight &l = pick_light(s, st, rr.code, j);
+                const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
+                V3 vtl = lp - isect.point;
+                const float dist = length(vtl);
+                vtl = normalize(vtl);
+                if (!(dot(isect.normal, vtl) > 0.0f)) continue;
+                const uint32_t pos = sbase + q++;
+                if (pos >= w.shadow_cap) { raise_error(s, MRT_ERR_LIMIT); break; }
+                ShadowRec sr;
+                sr.ox = isect.point.x; sr.oy = isect.point.y; sr.oz = isect.point.z;
+                sr.dx = vtl.x; sr.dy = vtl.y; sr.dz = vtl.z;
+                sr.dist = dist;
+                sr.node = idx;
+                sr.j = j;
+                sr.exclude = isect.prim;
+                w.shadows[pos] = sr;
+            }
+        }
+    }
+}
+
+template <int ACCEL, int MODE>
+__global__ void __launch_bounds__(128) k_wave_shadow(DevScene s, WaveState w, int level) {
+    const uint32_t n = min(w.levels[level].shadow_count, w.shadow_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const ShadowRec sr = w.shadows[i];
+        Ray r;
+        r.o = V3{sr.ox, sr.oy, sr.oz};
+        r.d = V3{sr.dx, sr.dy, sr.dz};
+        r.depth = 0;
+        r.exclude = sr.exclude;
+        if (scene_occ<ACCEL, MODE>(s, r, sr.dist)) atomicOr(&w.nodes[sr.node].occluded, 1u << (sr.j & 31u));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[1], (unsigned long long)n);
+}
+
+// bottom-up evaluation of one level: the shade() bodies after their recursive calls return
+__global__ void __launch_bounds__(128) k_wave_resolve(DevScene s, RenderParams p, WaveState w, int level) {
+    const Level L = clamp_level(w, w.levels[level]);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
+        const uint32_t idx = L.start + i;
+        const NodeRec nd = w.nodes[idx];
+        const RayRec rr = w.rays[idx];
+        V3 rgb{0.0f, 0.0f, 0.0f};
+        bool flag = false;
+        const uint32_t kind = nd.flags & 3u;
+        if (kind == kEmit) {
+            rgb = nd.point;
+            flag = true;
+        } else if (kind == kShaded) {
+            Task k;
+            uint32_t pixel, sample;
+            root_task(p, w, rr.root, k, pixel, sample);
+            const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+            V3 direct{0.0f, 0.0f, 0.0f};
+            const bool kd_pos = (nd.flags & kKdPos) != 0;
+            if (kd_pos && s.n_light > 0) {
+                for (uint32_t j = 0; j < p.spl; ++j) {
+                    const DevLight &l = pick_light(s, st, rr.code, j);
+                    const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
+                    const V3 vtl = normalize(lp - nd.point);
+                    const float c = dot(nd.normal, vtl);
+                    if (c > 0.0f && !((nd.occluded >> (j & 31u)) & 1u)) direct = direct + l.radiance.le * c;
+                }
+                direct = direct * nd.kd;
+                direct = direct / (float)p.spl;
+            }
+            if (p.shader == MRT_SHADER_WHITTED) {   // Whitted.cpp:64-106
+                rgb = direct;
+                if (nd.flags & kKsPos) rgb = rgb + nd.ks * nd.child[1];
+                if (nd.flags & kKtPos) rgb = rgb + nd.kt * nd.child[2];
+                rgb = rgb + nd.kd * 0.1f;
+            } else {   // PathTracer.cpp:100-163
+                V3 lid{0.0f, 0.0f, 0.0f}, lis{0.0f, 0.0f, 0.0f}, lit{0.0f, 0.0f, 0.0f};
+                if (nd.flags & kHasIndirect) {
+                    lid = lid + nd.kd * nd.child[0];
+                    if (nd.flags & kRRScaled) lid = lid / (0.5f * 0.5f);
+                    flag = (nd.child_flag & 1u) != 0;
+                    if (any_pos(direct) && flag) lid = V3{0.0f, 0.0f, 0.0f};
+                }
+                if (nd.flags & kKsPos) lis = lis + nd.ks * nd.child[1];
+                if (nd.flags & kKtPos) lit = lit + nd.kt * nd.child[2];
+                rgb = rgb + direct;
+                rgb = rgb + lid;
+                rgb = rgb + lis;
+                rgb = rgb + lit;
+            }
+        }
+        if (rr.parent == 0xFFFFFFFFu) {
+            w.root_rgb[rr.root] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
+        } else {
+            NodeRec &pn = w.nodes[rr.parent];
+            pn.child[rr.slot] = rgb;
+            if (flag) atomicOr(&pn.child_flag, 1u << rr.slot);
+        }
+    }
+}
+
+// fold the wave's per-sample values into the bitmap in sample order (Renderer.cpp:105-107)
+__global__ void k_wave_accumulate(RenderParams p, WaveState w) {
+    const uint32_t g0 = w.root_first, g1 = w.root_first + w.n_roots;
+    const uint32_t t0 = g0 / p.spp, t1 = (g1 - 1) / p.spp;
+    for (uint32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t <= t1; t += gridDim.x * blockDim.x) {
+        const Task k = task_of(p, p.task_base + t);
+        const uint32_t pixel = k.y * p.width + k.x;
+        uint32_t bm = p.bitmap[k.index];
+        float4 acc = p.accum ? p.accum[pixel] : make_float4(0, 0, 0, 0);
+        const uint32_t a = max(g0, t * p.spp), b = min(g1, (t + 1) * p.spp);
+        for (uint32_t g = a; g < b; ++g) {
+            const float4 c = w.root_rgb[g - g0];
+            const V3 rgb{c.x, c.y, c.z};
+            const uint32_t sample = p.spp_offset + (g - t * p.spp);
+            bm = incremental_avg(rgb, bm, sample + 1u);
+            acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
+        }
+        p.bitmap[k.index] = bm;
+        if (p.accum) p.accum[pixel] = acc;
+    }
+}
+
+// ============================== host orchestration ============================================
+struct TaskPlan {
+    bool implicit = true;
+    uint32_t n_tasks = 0;
+    std::vector<Task> list;                  // explicit tasks, block order
+    std::vector<uint32_t> round_first, round_count;
+};
+
+// Renderer ctor (Renderer.cpp:12-29) + renderScene block arithmetic (Renderer.cpp:79-93)
+bool plan_tasks(const MrtRenderOpts &o, uint32_t stride_px, TaskPlan &plan) {
+    const uint32_t w = o.width, h = o.height;
+    const uint32_t bsx = w / 16u, bsy = h / 16u;
+    if (bsx == 0 || bsy == 0) return false;
+    const uint32_t domain = (w / bsx) * (h / bsy);
+    const uint64_t res = (uint64_t)w * h;
+    std::vector<Task> tasks;
+    tasks.reserve((size_t)256 * bsx * bsy);
+    for (uint32_t i = 0; i < 256; ++i) {
+        const float block = halton(i, 2);
+        const uint32_t rb = (uint32_t)roundf(block * (float)domain);
+        const uint32_t pixel = (uint32_t)(((uint64_t)rb * bsx) % res);
+        const uint32_t sy = ((pixel / w) * bsy) % h;
+        for (uint32_t y = sy; y < sy + bsy; ++y) {
+            const uint32_t yw = y * stride_px;
+            const uint32_t sx = (pixel + yw) % w;
+            for (uint32_t x = sx; x < sx + bsx; ++x) tasks.push_back(Task{x, y, yw + x});
+        }
+    }
+    // the implicit rectangle?
+    const uint32_t rows = 16u * bsy;
+    bool rect = tasks.size() == (size_t)w * rows;
+    std::vector<uint8_t> seen((size_t)stride_px * h + 1, 0);
+    if (rect) {
+        for (const Task &t : tasks) {
+            if (t.x >= w || t.y >= rows || t.index != t.y * stride_px + t.x || seen[t.index]) { rect = false; break; }
+            seen[t.index] = 1;
+        }
+    }
+    if (rect) {
+        plan.implicit = true;
+        plan.n_tasks = w * rows;
+        plan.round_first = {0};
+        plan.round_count = {plan.n_tasks};
+        return true;
+    }
+    // explicit: drop tasks outside the bitmap (undefined behaviour in the reference), then rounds
+    // in which every pixel appears at most once, preserving block order per pixel
+    plan.implicit = false;
+    std::vector<uint32_t> visits((size_t)stride_px * h + 1, 0);
+    std::vector<std::vector<Task>> rounds;
+    for (const Task &t : tasks) {
+        if ((uint64_t)t.index >= (uint64_t)stride_px * h || t.x >= w) continue;
+        const uint32_t r = visits[t.index]++;
+        if (rounds.size() <= r) rounds.emplace_back();
+        rounds[r].push_back(t);
+    }
+    for (auto &r : rounds) {
+        plan.round_first.push_back((uint32_t)plan.list.size());
+        plan.round_count.push_back((uint32_t)r.size());
+        plan.list.insert(plan.list.end(), r.begin(), r.end());
+    }
+    plan.n_tasks = (uint32_t)plan.list.size();
+    return true;
+}
+
+template <int ACCEL, int MODE>
+void launch_noshadows(const DevScene &s, const RenderParams &p, uint32_t first, uint32_t count, int grid, cudaStream_t q) {
+    k_render_noshadows<ACCEL, MODE><<<grid, 128, 0, q>>>(s, p, first, count);
+}
+
+template <int ACCEL, int MODE>
+void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState &w, int level, int grid, cudaStream_t q) {
+    k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
+    k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
+    k_wave_shadow<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
+}
+
+#define MRT_DISPATCH(fn, accel, mode, ...)                                                                 \
+    do {                                                                                                    \
+        if ((accel) == MRT_ACCEL_NAIVE) fn<MRT_ACCEL_NAIVE, MRT_BVH_FAST>(__VA_ARGS__);                     \
+        else if ((accel) == MRT_ACCEL_REGULAR_GRID) fn<MRT_ACCEL_REGULAR_GRID, MRT_BVH_FAST>(__VA_ARGS__);  \
+        else if ((mode) == MRT_BVH_REFERENCE) fn<MRT_ACCEL_BVH, MRT_BVH_REFERENCE>(__VA_ARGS__);            \
+        else fn<MRT_ACCEL_BVH, MRT_BVH_FAST>(__VA_ARGS__);                                                  \
+    } while (0)
+
+uint32_t wave_roots_setting() {
+    static uint32_t v = [] {
+        const char *e = getenv("MRT_WAVE_ROOTS");
+        const long x = e ? atol(e) : (1l << 21);
+        return (uint32_t)std::max(1024l, std::min(x, 1l << 25));
+    }();
+    return v;
+}
+
+}  // namespace
+
+namespace mrt_host {
+
+static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
+                       float *d_accum, MrtRenderStats *stats, uint32_t strata) {
+    MrtContext *ctx = s->ctx;
+    cudaStream_t q = ctx->stream;
+    const uint32_t stride_px = stride / 4u;
+    TaskPlan plan;
+    if (!plan_tasks(*o, stride_px, plan)) {
+        set_error(ctx, "mrt_render: width and height must be at least 16 (Renderer block size width/16)");
+        return MRT_ERR_ARG;
+    }
+    RenderParams p{};
+    p.cam = make_camera(*cam);
+    p.width = o->width; p.height = o->height; p.spp = o->spp; p.spl = o->spl; p.stride_px = stride_px;
+    p.pixel_sampler = o->pixel_sampler; p.light_sampler = o->light_sampler; p.rr_sampler = o->rr_sampler;
+    p.shader = o->shader; p.constant_value = o->constant_value;
+    p.depth_min = o->depth_min; p.depth_max = o->depth_max;
+    p.seed = o->seed; p.spp_offset = o->spp_offset;
+    p.strata = strata;
+    p.bitmap = d_bitmap;
+    p.accum = (float4 *)d_accum;
+    p.inv_w = 1.0f / (float)o->width;   // Renderer.cpp:68-71
+    p.inv_h = 1.0f / (float)o->height;
+    p.pw = 0.5f / (float)o->width;
+    p.ph = 0.5f / (float)o->height;
+    p.n_tasks = plan.n_tasks;
+    int st = MRT_OK;
+    if (!plan.implicit) {
+        st = ensure(ctx, s->work[0], sizeof(Task) * plan.list.size());
+        if (st == MRT_OK)
+            st = cuda_status(ctx, cudaMemcpyAsync(s->work[0].ptr, plan.list.data(), sizeof(Task) * plan.list.size(),
+                                                  cudaMemcpyHostToDevice, q), "tasks");
+        if (st != MRT_OK) return st;
+        p.tasks = (const Task *)s->work[0].ptr;
+    }
+    if (plan.round_first.size() > 1 && o->spp > 1) {
+        // pixels revisited within a pass: the reference's pass-major order, one pass at a time
+        MrtRenderStats total{0, 0, 0, 0.0f};
+        for (uint32_t si = 0; si < o->spp; ++si) {
+            MrtRenderOpts one = *o;
+            one.spp = 1;
+            one.spp_offset = o->spp_offset + si;
+            MrtRenderStats part{};
+            st = render_impl(s, cam, &one, d_bitmap, stride, d_accum, &part, strata);
+            if (st != MRT_OK) return st;
+            total.rays_closest += part.rays_closest;
+            total.rays_shadow += part.rays_shadow;
+            total.paths += part.paths;
+            total.device_ms += part.device_ms;
+        }
+        if (stats) *stats = total;
+        return MRT_OK;
+    }
+    const int accel = s->opts.accelerator, mode = s->opts.bvh_mode;
+    const int grid = ctx->sm_count * 16;
+    uint64_t rays_closest = 0, rays_shadow = 0;
+    s->progress.store(0);
+    cudaEventRecord(ctx->ev0, q);
+    if (o->shader == MRT_SHADER_NOSHADOWS) {
+        for (size_t r = 0; r < plan.round_first.size(); ++r) {
+            if (s->stop.load()) return MRT_ERR_CANCELLED;
+            MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, plan.round_first[r], plan.round_count[r], grid, q);
+        }
+        rays_closest = (uint64_t)plan.n_tasks * o->spp;
+    } else {
+        if (o->spl > 32) { set_error(ctx, "mrt_render: samplesLight above 32 is not supported by the wavefront"); return MRT_ERR_ARG; }
+        uint64_t max_round = 0;
+        for (uint32_t c : plan.round_count) max_round = std::max<uint64_t>(max_round, c);
+        const uint32_t wave = (uint32_t)std::min<uint64_t>(max_round * o->spp, wave_roots_setting());
+        const int levels = std::max(1, o->depth_max + 1);
+        const uint64_t ray_cap = (uint64_t)wave * (uint64_t)(levels + 2);
+        const uint64_t shadow_cap = (uint64_t)wave * std::max(1u, o->spl) * 2ull;
+        if (ray_cap > 0xFFFFFFF0ull) { set_error(ctx, "mrt_render: wave too large"); return MRT_ERR_ARG; }
+        if (st == MRT_OK) st = ensure(ctx, s->work[1], sizeof(RayRec) * ray_cap);
+        if (st == MRT_OK) st = ensure(ctx, s->work[2], sizeof(NodeRec) * ray_cap);
+        if (st == MRT_OK) st = ensure(ctx, s->work[3], sizeof(ShadowRec) * shadow_cap);
+        if (st == MRT_OK) st = ensure(ctx, s->work[4], sizeof(Level) * (levels + 2));
+        if (st == MRT_OK) st = ensure(ctx, s->work[5], sizeof(float4) * wave);
+        if (st == MRT_OK) st = ensure(ctx, s->work[6], 16);
+        if (st != MRT_OK) return st;
+        WaveState w{};
+        w.rays = (RayRec *)s->work[1].ptr;
+        w.nodes = (NodeRec *)s->work[2].ptr;
+        w.shadows = (ShadowRec *)s->work[3].ptr;
+        w.levels = (Level *)s->work[4].ptr;
+        w.root_rgb = (float4 *)s->work[5].ptr;
+        w.counters = (unsigned long long *)s->work[6].ptr;
+        w.ray_cap = (uint32_t)ray_cap;
+        w.shadow_cap = (uint32_t)shadow_cap;
+        cudaMemsetAsync(w.counters, 0, 16, q);
+        for (size_t rd = 0; rd < plan.round_first.size(); ++rd) {
+            p.task_base = plan.round_first[rd];
+            const uint64_t total_roots = (uint64_t)plan.round_count[rd] * o->spp;
+            for (uint64_t r0 = 0; r0 < total_roots; r0 += wave) {
+                if (s->stop.load()) return MRT_ERR_CANCELLED;
+                w.root_first = (uint32_t)r0;
+                w.n_roots = (uint32_t)std::min<uint64_t>(wave, total_roots - r0);
+                cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
+                k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
+                for (int b = 0; b < levels; ++b) MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q);
+                for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
+                k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
+                s->progress.store((uint32_t)((r0 + w.n_roots) / std::max<uint64_t>(1, plan.round_count[rd])));
+            }
+        }
+        unsigned long long cnt[2] = {0, 0};
+        st = cuda_status(ctx, cudaMemcpyAsync(cnt, w.counters, 16, cudaMemcpyDeviceToHost, q), "counters");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "render");
+        rays_closest = cnt[0];
+        rays_shadow = cnt[1];
+    }
+    cudaEventRecord(ctx->ev1, q);
+    if (st == MRT_OK) st = cuda_status(ctx, cudaGetLastError(), "render kernels");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaEventSynchronize(ctx->ev1), "render");
+    if (st == MRT_OK) st = check_kernel_error(ctx);
+    s->progress.store(o->spp);
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->rays_closest = rays_closest;
+        stats->rays_shadow = rays_shadow;
+        stats->paths = (uint64_t)plan.n_tasks * o->spp;
+        stats->device_ms = ms;
+    }
+    return st;
+}
+
+int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
+           float *d_accum, MrtRenderStats *stats) {
+    return render_impl(s, cam, o, d_bitmap, stride, d_accum, stats, o->spp);
+}
+
+}  // namespace mrt_host
+
+extern "C" {
+
+int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *bitmap, uint32_t stride_bytes,
+               float *accum, uint32_t mem, MrtRenderStats *stats) {
+    if (!s || !cam || !o || !bitmap) return MRT_ERR_ARG;
+    MrtContext *ctx = s->ctx;
+    if (!s->built) { set_error(ctx, "mrt_render before mrt_scene_build"); return MRT_ERR_STATE; }
+    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_PATHTRACER || o->spp == 0 || o->spl == 0 ||
+        o->width < 16 || o->height < 16 || stride_bytes < 4u * o->width || cam->kind != MRT_CAMERA_PERSPECTIVE ||
+        o->pixel_sampler < 0 || o->pixel_sampler > 3 || o->light_sampler < 0 || o->light_sampler > 3 ||
+        o->rr_sampler < 0 || o->rr_sampler > 3) {
+        set_error(ctx, "mrt_render: invalid options");
+        return MRT_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    s->stop.store(0);
+    const size_t bm_bytes = (size_t)stride_bytes * o->height;
+    const size_t acc_bytes = 16ull * o->width * o->height;
+    uint32_t *d_bitmap = bitmap;
+    float *d_accum = accum;
+    int st = MRT_OK;
+    if (mem == MRT_MEM_HOST) {
+        st = ensure(ctx, s->work[7], bm_bytes + (accum ? acc_bytes : 0));
+        if (st != MRT_OK) return st;
+        d_bitmap = (uint32_t *)s->work[7].ptr;
+        d_accum = accum ? (float *)((char *)s->work[7].ptr + bm_bytes) : nullptr;
+        st = cuda_status(ctx, cudaMemcpyAsync(d_bitmap, bitmap, bm_bytes, cudaMemcpyHostToDevice, ctx->stream), "bitmap in");
+        if (st == MRT_OK && accum)
+            st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");
+        if (st != MRT_OK) return st;
+    }
+    st = render(s, cam, o, d_bitmap, stride_bytes, d_accum, stats);
+    if (st == MRT_OK && mem == MRT_MEM_HOST) {
+        st = cuda_status(ctx, cudaMemcpyAsync(bitmap, d_bitmap, bm_bytes, cudaMemcpyDeviceToHost, ctx->stream), "bitmap out");
+        if (st == MRT_OK && accum)
+            st = cuda_status(ctx, cudaMemcpyAsync(accum, d_accum, acc_bytes, cudaMemcpyDeviceToHost, ctx->stream), "accum out");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "render copy out");
+    }
+    return st;
+}
+
+void mrt_render_stop(MrtScene *s) {
+    if (s) s->stop.store(1);
+}
+
+uint32_t mrt_render_progress(const MrtScene *s) { return s ? s->progress.load() : 0u; }
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+"""Whole-frame parity of mrt_render (Renderer::renderFrame on the device) against the oracle's
+restatement of the renderer with the same keyed sample stream (GPU).
+
+NoShadows, Whitted and PathTracer frames must equal the oracle bit for bit: the ARGB8888 bitmap
+(incrementalAvg of every sample, Utils.cpp:48-70) and the fp32 per-pixel sums.  The tolerance the
+specification allows (1e-4 for the deterministic shaders, 1e-3 for PathTracer radiance) is asserted
+on the fp32 sums as the documented bound; the bitmaps are compared exactly.
+"""
+import numpy as np
+import pytest
+
+import orc as O
+from mobileraytracer_b200 import Scene, capi, scenes
+
+pytestmark = pytest.mark.gpu
+
+NS, WH, PT = capi.MRT_SHADER_NOSHADOWS, capi.MRT_SHADER_WHITTED, capi.MRT_SHADER_PATHTRACER
+GPU_ACCELS = [  # (gpu accelerator, bvh mode, oracle accelerator with the same answers)
+    (capi.MRT_ACCEL_NAIVE, capi.MRT_BVH_FAST, 0),
+    (capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST, 1),
+    (capi.MRT_ACCEL_BVH, capi.MRT_BVH_REFERENCE, 2),
+    (capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST, 3),
+]
+
+
+def render_both(ctx, sc, cam, opts, accel, mode, oacc):
+    g = Scene(ctx, sc).build(accel, mode, camera_position=list(cam.position))
+    bm_g, acc_g, stats = g.render(cam, opts, accum=np.zeros((opts.height, opts.width, 4), np.float32))
+    o = O.OrcScene(sc, oacc, camera_position=list(cam.position))
+    bm_o, acc_o, counts = o.render(cam, opts)
+    return bm_g, acc_g, stats, bm_o, acc_o, counts
+
+
+def assert_same(bm_g, acc_g, bm_o, acc_o, tol):
+    diff = np.abs(acc_g[..., :3] - acc_o[..., :3])
+    assert float(diff.max()) <= tol, f"max |radiance difference| {diff.max()}"
+    nd = int(np.sum(bm_g != bm_o))
+    assert nd == 0, f"{nd} bitmap pixels differ (max radiance diff {diff.max()})"
+
+
+@pytest.mark.parametrize("accel,mode,oacc", GPU_ACCELS)
+def test_noshadows_soup(ctx, accel, mode, oacc):
+    sc = scenes.triangle_soup(30000, 2, 320, 240)
+    opts = capi.render_opts(shader=NS, width=320, height=240, spp=1, spl=1)
+    bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, accel, mode, oacc)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-4)
+    assert stats.rays_closest == counts[0]
+
+
+@pytest.mark.parametrize("shader", [NS, WH, PT])
+@pytest.mark.parametrize("accel,mode,oacc", GPU_ACCELS)
+def test_glass_room_all_shaders(ctx, shader, accel, mode, oacc):
+    """planes + spheres (mirror, glass ior 1.9, diffuse+specular) + triangles + 2 area lights."""
+    sc = scenes.glass_room()
+    opts = capi.render_opts(shader=shader, width=96, height=64, spp=3, spl=2, seed=7)
+    bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, accel, mode, oacc)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3 if shader == PT else 1e-4)
+    assert stats.rays_closest == counts[0] and stats.rays_shadow == counts[1]
+
+
+def test_config1_cornell_whitted(ctx):
+    """Config 1: Whitted, 256x256, 1 spp, Constant(0.5) camera sampler, BVH."""
+    sc = scenes.cornell_box()
+    opts = capi.render_opts(shader=WH, width=256, height=256, spp=1, spl=1, seed=1)
+    for accel, mode, oacc in ((capi.MRT_ACCEL_BVH, capi.MRT_BVH_REFERENCE, 2), (capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST, 3)):
+        bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, accel, mode, oacc)
+        assert_same(bm_g, acc_g, bm_o, acc_o, 1e-4)
+        assert np.count_nonzero(bm_g & 0xFFFFFF) > 256 * 256 // 2
+
+
+@pytest.mark.parametrize("sampler", [capi.MRT_SAMPLER_STRATIFIED, capi.MRT_SAMPLER_HALTON, capi.MRT_SAMPLER_RANDOM])
+def test_pathtracer_samplers_rr(ctx, sampler):
+    """PathTracer with Russian roulette beyond depth 3, max depth 6 (config 3's setting) and every
+    sampler kind on the camera jitter, the light positions and the roulette."""
+    sc = scenes.cornell_box()
+    opts = capi.render_opts(shader=PT, width=64, height=64, spp=8, spl=1, pixel_sampler=sampler,
+                            light_sampler=sampler, rr_sampler=sampler, depth_min=3, depth_max=6, seed=3)
+    bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, capi.MRT_ACCEL_BVH,
+                                                          capi.MRT_BVH_FAST, 3)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3)
+
+
+def test_config3_heightfield_crop(ctx):
+    """Config 3 scene (524,288-triangle fBm terrain, 4 area quads) at 64x64, 4 spp HaltonSeq,
+    depth 6, RR after 3: per-pixel radiance within 1e-3 of the oracle (asserted: exact)."""
+    sc = scenes.heightfield(512, 1, width=64, height=64)
+    opts = capi.render_opts(shader=PT, width=64, height=64, spp=4, spl=1, pixel_sampler=capi.MRT_SAMPLER_HALTON,
+                            light_sampler=capi.MRT_SAMPLER_HALTON, rr_sampler=capi.MRT_SAMPLER_HALTON,
+                            depth_min=3, depth_max=6, seed=1)
+    bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, capi.MRT_ACCEL_BVH,
+                                                          capi.MRT_BVH_FAST, 3)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3)
+
+
+def test_progressive_continuation(ctx):
+    """spp_offset continues the stream and the running mean: 2 + 2 samples == 4 samples."""
+    sc = scenes.glass_room()
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH)
+    o4 = capi.render_opts(shader=PT, width=48, height=48, spp=4, spl=1, seed=5)
+    bm4, _, _ = g.render(sc.camera, o4)
+    bm = np.zeros((48, 48), np.uint32)
+    g.render(sc.camera, capi.render_opts(shader=PT, width=48, height=48, spp=2, spl=1, seed=5), bitmap=bm)
+    o2b = capi.render_opts(shader=PT, width=48, height=48, spp=2, spl=1, seed=5, spp_offset=2)
+    o2b.spp = 2
+    # the stratified count must be the full render's for Stratified; Random/Constant do not use it
+    g.render(sc.camera, o2b, bitmap=bm)
+    assert (bm == bm4).all()
+
+
+def test_odd_sizes_and_stride(ctx):
+    """Width not a multiple of 16 (blocks overlap / leave gaps exactly as the reference's block
+    arithmetic does) and a padded row pitch."""
+    sc = scenes.glass_room()
+    for w, h in ((100, 50), (37, 29)):
+        for shader in (NS, WH):
+            opts = capi.render_opts(shader=shader, width=w, height=h, spp=2, spl=1, seed=2)
+            bm_g, acc_g, _, bm_o, acc_o, _ = render_both(ctx, sc, sc.camera, opts, capi.MRT_ACCEL_BVH,
+                                                         capi.MRT_BVH_REFERENCE, 2)
+            assert (bm_g == bm_o).all(), (w, h, shader)
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH)
+    opts = capi.render_opts(shader=NS, width=64, height=32, spp=1)
+    padded = np.full((32, 80), 0xDEADBEEF, np.uint32)
+    g.render(sc.camera, opts, bitmap=padded, stride_bytes=80 * 4)
+    plain, _, _ = g.render(sc.camera, opts)
+    assert (padded[:, :64] == plain).all() and (padded[:, 64:] == 0xDEADBEEF).all()
+
+
+def test_errors_are_reported(ctx):
+    import mobileraytracer_b200 as m
+    sc = scenes.glass_room()
+    g = Scene(ctx, sc)
+    with pytest.raises(m.MrtError) as e:
+        g.render(sc.camera, capi.render_opts(width=32, height=32))
+    assert e.value.status == capi.MRT_ERR_STATE
+    g.build(capi.MRT_ACCEL_BVH)
+    with pytest.raises(m.MrtError) as e:
+        g.render(sc.camera, capi.render_opts(width=8, height=8))
+    assert e.value.status == capi.MRT_ERR_ARG
+    bad = capi.render_opts(width=32, height=32)
+    bad.shader = 9
+    with pytest.raises(m.MrtError):
+        g.render(sc.camera, bad)
+    ok, _, _ = g.render(sc.camera, capi.render_opts(width=32, height=32))   # context still usable
+    assert ok.any()
