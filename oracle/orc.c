@@ -578,6 +578,8 @@ static void grid_build(Grid *g, const PrimSet *ps, Box bounds, int32_t G, int in
             y1 = y1 > 0 ? y1 : 0; y2 = (G - 1 < y2) ? G - 1 : y2; y2 = fabsf(sy) < EPS ? 0 : y2; y1 = (y1 < y2) ? y1 : y2;
             int32_t z1 = (int32_t)((bd.mn.z - bounds.mn.z) * rz), z2 = (int32_t)((bd.mx.z - bounds.mn.z) * rz) + 1;
             z1 = z1 > 0 ? z1 : 0; z2 = (G - 1 < z2) ? G - 1 : z2; z2 = fabsf(sz) < EPS ? 0 : z2; z1 = (z1 < z2) ? z1 : z2;
+            /* a NaN box gives negative cell indices (undefined behaviour in the reference): skipped */
+            if (x1 < 0 || y1 < 0 || z1 < 0 || x2 < 0 || y2 < 0 || z2 < 0) continue;
             for (int32_t x = x1; x <= x2; ++x)
                 for (int32_t y = y1; y <= y2; ++y)
                     for (int32_t z = z1; z <= z2; ++z) {
