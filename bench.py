@@ -313,6 +313,7 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    scene.close()
     ctx.close()
     if ws > 1:
         torch.distributed.destroy_process_group()

@@ -13,6 +13,7 @@ device and raises MrtError when the library or the GPU is unavailable.
 from __future__ import annotations
 
 import ctypes
+import weakref
 
 import numpy as np
 
@@ -54,6 +55,7 @@ class Context:
             raise MrtError(st, f"mrt_context_create(device={device}) failed")
         self.h = h
         self.device = device
+        self._scenes = weakref.WeakSet()
 
     def check(self, st: int, what: str):
         if st != capi.MRT_OK:
@@ -67,7 +69,10 @@ class Context:
         return int(self.lib.mrt_context_stream(self.h) or 0)
 
     def close(self):
+        """Destroys the context; scenes still open on it are destroyed first."""
         if getattr(self, "h", None):
+            for s in list(getattr(self, "_scenes", ())):
+                s.close()
             self.lib.mrt_context_destroy(self.h)
             self.h = None
 
@@ -87,8 +92,11 @@ class Scene:
         self.host = scene
         self._desc = scene.desc()
         h = ctypes.c_void_p()
+        if not ctx.h:
+            raise MrtError(capi.MRT_ERR_STATE, "context is closed")
         ctx.check(self.lib.mrt_scene_create(ctx.h, ctypes.byref(self._desc), ctypes.byref(h)), "mrt_scene_create")
         self.h = h
+        ctx._scenes.add(self)
 
     def build(self, accelerator: int = capi.MRT_ACCEL_BVH, bvh_mode: int = capi.MRT_BVH_FAST, grid_size: int = 0,
               grid_index: int = capi.MRT_GRID_INDEX_REFERENCE, camera_position=None):
@@ -172,7 +180,8 @@ class Scene:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.mrt_scene_destroy(self.h)
+            if self.ctx.h:   # a closed context already destroyed its scenes
+                self.lib.mrt_scene_destroy(self.h)
             self.h = None
 
     def __del__(self):

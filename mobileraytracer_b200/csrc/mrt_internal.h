@@ -55,6 +55,11 @@ struct MrtScene {
     std::atomic<uint32_t> progress{0};
     std::atomic<int> stop{0};
     DevBuf work[8];                     // render scratch (wavefront pools, per-pixel buffers)
+    void *plan_cache = nullptr;         // pixel schedule of the last (width, height, pitch)
+    void (*plan_cache_free)(void *) = nullptr;
+    ~MrtScene() {
+        if (plan_cache && plan_cache_free) plan_cache_free(plan_cache);
+    }
 };
 
 namespace mrt_host {

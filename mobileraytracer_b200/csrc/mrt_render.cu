@@ -60,6 +60,13 @@ __device__ __forceinline__ Task task_of(const RenderParams &p, uint32_t t) {
     return k;
 }
 
+// fp32 sum slot of the bitmap pixel a task writes (a task past the right edge wraps into the next
+// row, as pixelIndex = y * stride + x does in Renderer.cpp:105); -1 when it lands in the row padding
+__device__ __forceinline__ int64_t accum_slot(const RenderParams &p, const Task &k) {
+    const uint32_t row = k.index / p.stride_px, col = k.index - row * p.stride_px;
+    return col < p.width ? (int64_t)row * p.width + col : -1;
+}
+
 __device__ __forceinline__ Ray primary_ray(const RenderParams &p, const Task &k, const Stream &st) {
     const float u = (float)k.x * p.inv_w, v = (float)k.y * p.inv_h;   // Renderer.cpp:95-99
     const float r1 = draw(st, p.pixel_sampler, 0u, 0u);
@@ -121,8 +128,9 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
         const uint32_t t = round_first + i;
         const Task k = task_of(p, t);
         const uint32_t pixel = k.y * p.width + k.x;
+        const int64_t slot = p.accum ? accum_slot(p, k) : -1;
         uint32_t bm = p.bitmap[k.index];
-        float4 acc = p.accum ? p.accum[pixel] : make_float4(0, 0, 0, 0);
+        float4 acc = slot >= 0 ? p.accum[slot] : make_float4(0, 0, 0, 0);
         for (uint32_t si = 0; si < p.spp; ++si) {
             const uint32_t sample = p.spp_offset + si;
             const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
@@ -138,7 +146,7 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
             acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
         }
         p.bitmap[k.index] = bm;
-        if (p.accum) p.accum[pixel] = acc;
+        if (slot >= 0) p.accum[slot] = acc;
     }
 }
 
@@ -506,9 +514,9 @@ __global__ void k_wave_accumulate(RenderParams p, WaveState w) {
     const uint32_t t0 = g0 / p.spp, t1 = (g1 - 1) / p.spp;
     for (uint32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t <= t1; t += gridDim.x * blockDim.x) {
         const Task k = task_of(p, p.task_base + t);
-        const uint32_t pixel = k.y * p.width + k.x;
+        const int64_t slot = p.accum ? accum_slot(p, k) : -1;
         uint32_t bm = p.bitmap[k.index];
-        float4 acc = p.accum ? p.accum[pixel] : make_float4(0, 0, 0, 0);
+        float4 acc = slot >= 0 ? p.accum[slot] : make_float4(0, 0, 0, 0);
         const uint32_t a = max(g0, t * p.spp), b = min(g1, (t + 1) * p.spp);
         for (uint32_t g = a; g < b; ++g) {
             const float4 c = w.root_rgb[g - g0];
@@ -518,12 +526,14 @@ __global__ void k_wave_accumulate(RenderParams p, WaveState w) {
             acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
         }
         p.bitmap[k.index] = bm;
-        if (p.accum) p.accum[pixel] = acc;
+        if (slot >= 0) p.accum[slot] = acc;
     }
 }
 
 // ============================== host orchestration ============================================
 struct TaskPlan {
+    uint32_t width = 0, height = 0, stride_px = 0;
+    bool uploaded = false;               // explicit list already in the scene's work[0]
     bool implicit = true;
     uint32_t n_tasks = 0;
     std::vector<Task> list;                  // explicit tasks, block order
@@ -573,7 +583,7 @@ bool plan_tasks(const MrtRenderOpts &o, uint32_t stride_px, TaskPlan &plan) {
     std::vector<uint32_t> visits((size_t)stride_px * h + 1, 0);
     std::vector<std::vector<Task>> rounds;
     for (const Task &t : tasks) {
-        if ((uint64_t)t.index >= (uint64_t)stride_px * h || t.x >= w) continue;
+        if ((uint64_t)t.index >= (uint64_t)stride_px * h) continue;   // outside the bitmap
         const uint32_t r = visits[t.index]++;
         if (rounds.size() <= r) rounds.emplace_back();
         rounds[r].push_back(t);
@@ -585,6 +595,23 @@ bool plan_tasks(const MrtRenderOpts &o, uint32_t stride_px, TaskPlan &plan) {
     }
     plan.n_tasks = (uint32_t)plan.list.size();
     return true;
+}
+
+TaskPlan *cached_plan(MrtScene *s, uint32_t w, uint32_t h, uint32_t stride_px) {
+    TaskPlan *p = static_cast<TaskPlan *>(s->plan_cache);
+    if (p && p->width == w && p->height == h && p->stride_px == stride_px) return p;
+    delete p;
+    p = new TaskPlan();
+    p->width = w;
+    p->height = h;
+    p->stride_px = stride_px;
+    MrtRenderOpts o{};
+    o.width = w;
+    o.height = h;
+    if (!plan_tasks(o, stride_px, *p)) p->n_tasks = 0;
+    s->plan_cache = p;
+    s->plan_cache_free = [](void *q) { delete static_cast<TaskPlan *>(q); };
+    return p;
 }
 
 template <int ACCEL, int MODE>
@@ -625,8 +652,9 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     MrtContext *ctx = s->ctx;
     cudaStream_t q = ctx->stream;
     const uint32_t stride_px = stride / 4u;
-    TaskPlan plan;
-    if (!plan_tasks(*o, stride_px, plan)) {
+    // the block schedule depends only on (width, height, row pitch): planned once per scene
+    TaskPlan &plan = *cached_plan(s, o->width, o->height, stride_px);
+    if (plan.n_tasks == 0) {
         set_error(ctx, "mrt_render: width and height must be at least 16 (Renderer block size width/16)");
         return MRT_ERR_ARG;
     }
@@ -647,11 +675,14 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     p.n_tasks = plan.n_tasks;
     int st = MRT_OK;
     if (!plan.implicit) {
-        st = ensure(ctx, s->work[0], sizeof(Task) * plan.list.size());
-        if (st == MRT_OK)
-            st = cuda_status(ctx, cudaMemcpyAsync(s->work[0].ptr, plan.list.data(), sizeof(Task) * plan.list.size(),
-                                                  cudaMemcpyHostToDevice, q), "tasks");
-        if (st != MRT_OK) return st;
+        if (!plan.uploaded) {
+            st = ensure(ctx, s->work[0], sizeof(Task) * plan.list.size());
+            if (st == MRT_OK)
+                st = cuda_status(ctx, cudaMemcpyAsync(s->work[0].ptr, plan.list.data(), sizeof(Task) * plan.list.size(),
+                                                      cudaMemcpyHostToDevice, q), "tasks");
+            if (st != MRT_OK) return st;
+            plan.uploaded = true;
+        }
         p.tasks = (const Task *)s->work[0].ptr;
     }
     if (plan.round_first.size() > 1 && o->spp > 1) {

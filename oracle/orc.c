@@ -1395,15 +1395,16 @@ static Task *block_tasks(uint32_t w, uint32_t h, uint32_t real_w, uint32_t *coun
     return t;
 }
 
-typedef struct { const OrcScene *s; const Cam *cam; const MrtRenderOpts *o; const Task *tasks; uint32_t *bitmap; float *accum; uint32_t sample; } RenderJob;
+typedef struct { const OrcScene *s; const Cam *cam; const MrtRenderOpts *o; const Task *tasks; uint32_t *bitmap; float *accum; uint32_t sample; uint32_t real_w; } RenderJob;
 static void render_body(long k, void *vctx, uint64_t *cnt) {
     RenderJob *j = (RenderJob *)vctx;
     const Task *t = &j->tasks[k];
     const V3 rgb = pixel_sample(j->s, j->cam, j->o, t->x, t->y, j->sample, &cnt[0], &cnt[1]);
     const float c3[3] = {rgb.x, rgb.y, rgb.z};
     j->bitmap[t->index] = orc_incremental_avg(c3, j->bitmap[t->index], j->sample + 1u);
-    if (j->accum) {
-        float *a = j->accum + 4 * ((size_t)t->y * j->o->width + t->x);
+    const uint32_t row = t->index / j->real_w, col = t->index % j->real_w;
+    if (j->accum && col < j->o->width) {
+        float *a = j->accum + 4 * ((size_t)row * j->o->width + col);
         a[0] += rgb.x; a[1] += rgb.y; a[2] += rgb.z; a[3] += 1.0f;
     }
 }
@@ -1433,13 +1434,14 @@ int orc_render(OrcScene *s, const MrtCamera *camera, const MrtRenderOpts *o, uin
                 const V3 rgb = pixel_sample(s, &cam, o, tasks[k].x, tasks[k].y, sample, &nc, &ns);
                 const float c3[3] = {rgb.x, rgb.y, rgb.z};
                 bitmap[tasks[k].index] = orc_incremental_avg(c3, bitmap[tasks[k].index], sample + 1u);
-                if (accum && tasks[k].x < o->width) {
-                    float *a = accum + 4 * ((size_t)tasks[k].y * o->width + tasks[k].x);
+                const uint32_t row = tasks[k].index / real_w, col = tasks[k].index % real_w;
+                if (accum && col < o->width) {   /* the fp32 sum of the bitmap pixel written */
+                    float *a = accum + 4 * ((size_t)row * o->width + col);
                     a[0] += rgb.x; a[1] += rgb.y; a[2] += rgb.z; a[3] += 1.0f;
                 }
             }
         } else {
-            RenderJob j; j.s = s; j.cam = &cam; j.o = o; j.tasks = tasks; j.bitmap = bitmap; j.accum = accum; j.sample = sample;
+            RenderJob j; j.s = s; j.cam = &cam; j.o = o; j.tasks = tasks; j.bitmap = bitmap; j.accum = accum; j.sample = sample; j.real_w = real_w;
             uint64_t cnt[2];
             par_for((long)nt, threads, 64, render_body, &j, cnt);
             nc += cnt[0]; ns += cnt[1];
