@@ -60,6 +60,8 @@ class ClockSampler:
         self.path = None
 
     def __enter__(self):
+        """Starts sampling and waits for the first sample: nvidia-smi's start-up can hold the driver
+        for a moment, which must not fall inside the timed region."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -68,8 +70,18 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
-        time.sleep(0.15)
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 20 and os.path.getsize(self.path) == 0:
+            time.sleep(0.05)
+        self.first = 0
         return self
+
+    def mark(self):
+        """Only samples after this call count (the start of the timed region)."""
+        try:
+            self.first = sum(1 for _ in open(self.path))
+        except OSError:
+            self.first = 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -84,7 +96,9 @@ class ClockSampler:
             return None
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for k, line in enumerate(open(self.path)):
+            if k < self.first:
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -243,19 +257,21 @@ def main():
         _, _, st = scene.render(sc.camera, opts, bitmap=bitmap)
         return st
 
+    clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     dev_ms, rays = 0.0, 0
+    clocks.mark()
     wall0 = time.perf_counter()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            st = step()
-            dev_ms += st.device_ms
-            rays += st.rays_closest
+    for _ in range(args.steps):
+        st = step()
+        dev_ms += st.device_ms
+        rays += st.rays_closest
     torch.cuda.synchronize()
+    clocks.__exit__(None, None, None)
     wall = time.perf_counter() - wall0
     if ws > 1:
         t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)

@@ -65,6 +65,25 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
     return OUT
 
 
+DROPIN_SRC = os.path.join(HERE, "cpp", "src", "dropin.cpp")
+DROPIN_OUT = os.path.join(OUT_DIR, "libmrt_dropin.so")
+
+
+def build_dropin(verbose: bool = False, force: bool = False) -> str:
+    """libmrt_dropin.so: the MobileRT C++ API (cpp/include) over libmrt_cuda.so."""
+    lib = build(verbose=verbose)
+    deps = [DROPIN_SRC, lib, os.path.join(HERE, "cpp", "include", "MobileRT", "b200_api.hpp")]
+    if not force and os.path.exists(DROPIN_OUT) and all(os.path.getmtime(d) <= os.path.getmtime(DROPIN_OUT) for d in deps):
+        return DROPIN_OUT
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+           "-I", os.path.join(HERE, "cpp", "include"), "-I", os.path.join(HERE, "cpp", "glm_min"),
+           DROPIN_SRC, "-L", OUT_DIR, "-lmrt_cuda", "-Wl,-rpath,$ORIGIN", "-o", DROPIN_OUT]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return DROPIN_OUT
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--verbose", action="store_true")
@@ -72,3 +91,4 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(a.verbose, a.ptxas_info, a.force or a.ptxas_info))
+    print(build_dropin(a.verbose, a.force))

@@ -1,0 +1,3 @@
+// PointLight.hpp - same path as the reference header (app/Components/Lights/PointLight.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

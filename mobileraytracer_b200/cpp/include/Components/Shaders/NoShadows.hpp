@@ -1,0 +1,3 @@
+// NoShadows.hpp - same path as the reference header (app/Components/Shaders/NoShadows.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

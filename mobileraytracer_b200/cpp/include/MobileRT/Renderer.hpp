@@ -1,0 +1,3 @@
+// Renderer.hpp - same path as the reference header (app/MobileRT/Renderer.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

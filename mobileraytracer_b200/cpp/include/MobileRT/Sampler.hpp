@@ -1,0 +1,3 @@
+// Sampler.hpp - same path as the reference header (app/MobileRT/Sampler.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

@@ -1,0 +1,3 @@
+// Scene.hpp - same path as the reference header (app/MobileRT/Scene.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

@@ -1,0 +1,3 @@
+// Shader.hpp - same path as the reference header (app/MobileRT/Shader.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

@@ -1,0 +1,3 @@
+// Sphere.hpp - same path as the reference header (app/MobileRT/Shapes/Sphere.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

@@ -1,0 +1,3 @@
+// Utils.hpp - same path as the reference header (app/MobileRT/Utils.hpp); the classes live in b200_api.hpp.
+#pragma once
+#include "MobileRT/b200_api.hpp"

@@ -353,9 +353,18 @@ static int stage_in(MrtContext *ctx, DevBuf &b, const void *src, size_t bytes) {
     return cuda_status(ctx, cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream), "copy in");
 }
 
+// device buffers are read and written with vector accesses: rays as two 16-byte loads, hits as
+// one 8-byte store, per-ray counters and distances as 4-byte words
+static bool misaligned(MrtContext *ctx, uint32_t mem, const void *p, uintptr_t align, const char *what) {
+    if (mem != MRT_MEM_DEVICE || ((uintptr_t)p & (align - 1)) == 0) return false;
+    set_error(ctx, "%s must be %u-byte aligned", what, (unsigned)align);
+    return true;
+}
+
 int mrt_trace_closest(MrtScene *s, const MrtRay *rays, uint32_t n, MrtHit *hits, uint32_t mem) {
     if (!s || (n && (!rays || !hits))) return MRT_ERR_ARG;
     MrtContext *ctx = s->ctx;
+    if (misaligned(ctx, mem, rays, 16, "rays") || misaligned(ctx, mem, hits, 8, "hits")) return MRT_ERR_ARG;
     if (!s->built) { set_error(ctx, "mrt_trace_closest before mrt_scene_build"); return MRT_ERR_STATE; }
     if (n == 0) return MRT_OK;
     cudaSetDevice(ctx->device);
@@ -379,6 +388,7 @@ int mrt_trace_closest(MrtScene *s, const MrtRay *rays, uint32_t n, MrtHit *hits,
 int mrt_trace_any(MrtScene *s, const MrtRay *rays, const float *dist, uint32_t n, uint8_t *occluded, uint32_t mem) {
     if (!s || (n && (!rays || !dist || !occluded))) return MRT_ERR_ARG;
     MrtContext *ctx = s->ctx;
+    if (misaligned(ctx, mem, rays, 16, "rays") || misaligned(ctx, mem, dist, 4, "dist")) return MRT_ERR_ARG;
     if (!s->built) { set_error(ctx, "mrt_trace_any before mrt_scene_build"); return MRT_ERR_STATE; }
     if (n == 0) return MRT_OK;
     cudaSetDevice(ctx->device);
@@ -406,6 +416,9 @@ int mrt_trace_closest_counts(MrtScene *s, const MrtRay *rays, uint32_t n, uint32
                              uint32_t mem) {
     if (!s || (n && (!rays || !node_fetch || !tri_fetch))) return MRT_ERR_ARG;
     MrtContext *ctx = s->ctx;
+    if (misaligned(ctx, mem, rays, 16, "rays") || misaligned(ctx, mem, node_fetch, 4, "node_fetch") ||
+        misaligned(ctx, mem, tri_fetch, 4, "tri_fetch"))
+        return MRT_ERR_ARG;
     if (!s->built) { set_error(ctx, "mrt_trace_closest_counts before mrt_scene_build"); return MRT_ERR_STATE; }
     if (s->opts.accelerator != MRT_ACCEL_BVH || s->opts.bvh_mode != MRT_BVH_FAST) {
         set_error(ctx, "mrt_trace_closest_counts: only the FAST BVH has a counting replay");

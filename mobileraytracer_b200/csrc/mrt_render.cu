@@ -802,14 +802,20 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
     s->stop.store(0);
     const size_t bm_bytes = (size_t)stride_bytes * o->height;
     const size_t acc_bytes = 16ull * o->width * o->height;
+    const size_t acc_offset = (bm_bytes + 255) & ~(size_t)255;   // the sums are read as float4
     uint32_t *d_bitmap = bitmap;
     float *d_accum = accum;
     int st = MRT_OK;
+    if (mem == MRT_MEM_DEVICE && (((uintptr_t)bitmap & 3u) || ((uintptr_t)accum & 15u) || (stride_bytes & 3u))) {
+        set_error(ctx, "mrt_render: the bitmap must be 4-byte aligned (and the row pitch a multiple of 4) and the "
+                       "sums 16-byte aligned");
+        return MRT_ERR_ARG;
+    }
     if (mem == MRT_MEM_HOST) {
-        st = ensure(ctx, s->work[7], bm_bytes + (accum ? acc_bytes : 0));
+        st = ensure(ctx, s->work[7], acc_offset + (accum ? acc_bytes : 0));
         if (st != MRT_OK) return st;
         d_bitmap = (uint32_t *)s->work[7].ptr;
-        d_accum = accum ? (float *)((char *)s->work[7].ptr + bm_bytes) : nullptr;
+        d_accum = accum ? (float *)((char *)s->work[7].ptr + acc_offset) : nullptr;
         st = cuda_status(ctx, cudaMemcpyAsync(d_bitmap, bitmap, bm_bytes, cudaMemcpyHostToDevice, ctx->stream), "bitmap in");
         if (st == MRT_OK && accum)
             st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");
