@@ -308,7 +308,7 @@ def main():
             "peak_source": peak_kind, "traffic": (tpr * len(rays_np)) if tpr else None,
             "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": alg_bytes / len(rays_np),
             "node_records_per_ray": float(nodes.mean()), "tri_records_per_ray": float(tris.mean()),
-            "kernel": "k_render_noshadows<BVH,FAST>"}
+            "kernel": "k_render_noshadows_fast (persistent)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

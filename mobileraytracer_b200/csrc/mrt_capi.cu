@@ -122,6 +122,7 @@ int mrt_context_create(int device, MrtContext **out) {
     if (st == MRT_OK) st = cuda_status(ctx, cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device), "attr");
     if (st == MRT_OK) st = cuda_status(ctx, cudaMalloc(&ctx->d_error, sizeof(int32_t)), "cudaMalloc");
     if (st == MRT_OK) st = cuda_status(ctx, cudaMemset(ctx->d_error, 0, sizeof(int32_t)), "memset");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaMalloc(&ctx->d_counters, 64 * sizeof(uint32_t)), "cudaMalloc");
     if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&ctx->ev0), "event");
     if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&ctx->ev1), "event");
     if (st != MRT_OK) {
@@ -139,6 +140,7 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto &b : ctx->scratch) dev_free(b);
     if (ctx->d_error) cudaFree(ctx->d_error);
+    if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -23,6 +23,7 @@ struct MrtContext {
     std::string error;
     int sm_count = 148;
     int32_t *d_error = nullptr;         // device error flag (MRT_ERR_LIMIT from kernels)
+    uint32_t *d_counters = nullptr;     // work counters of the persistent kernels (64 slots)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];

@@ -2,7 +2,7 @@
 // mrt_trace_closest_counts.  One thread per ray; rays are 32-byte MrtRay records read as two
 // 128-bit loads.
 #include "mrt_internal.h"
-#include "mrt_trace.cuh"
+#include "mrt_persistent.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
@@ -59,6 +59,42 @@ __global__ void __launch_bounds__(128) k_trace_counts(DevScene s, const MrtRay *
     }
 }
 
+// persistent FAST-BVH versions: work items are rays of the input array
+struct TraceLane {
+    uint32_t i;
+};
+template <bool kCount>
+struct TraceWork {
+    const MrtRay *rays;
+    MrtHit *hits;
+    uint32_t *nodes, *tris;
+    uint32_t n;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return n; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ bool begin(uint32_t item, TraceLane &lane, Ray &r) const {
+        lane.i = item;
+        r = load_ray(rays, item);
+        return true;
+    }
+    __device__ bool finish(TraceLane &lane, Ray &, bool hit, float t, uint32_t id, const FastTrav &tr) const {
+        if (kCount) {
+            nodes[lane.i] = tr.c_nodes;
+            tris[lane.i] = tr.c_tris;
+        } else {
+            reinterpret_cast<uint2 *>(hits)[lane.i] =
+                make_uint2(__float_as_uint(hit ? t : kRayLengthMax), hit ? id : MRT_HIT_NONE);
+        }
+        return false;
+    }
+};
+
+template <bool kCount>
+__global__ void __launch_bounds__(128) k_trace_persistent(DevScene s, TraceWork<kCount> work) {
+    TraceLane lane;
+    persistent_closest<kCount>(s, work, lane);
+}
+
 template <int ACCEL, int MODE>
 void launch_closest(const DevScene &s, const MrtRay *rays, uint32_t n, MrtHit *hits, int grid, cudaStream_t q) {
     k_trace_closest<ACCEL, MODE><<<grid, 128, 0, q>>>(s, rays, n, hits);
@@ -86,8 +122,20 @@ int grid_for(const MrtContext *ctx, uint32_t n) {
 
 namespace mrt_host {
 
+int persistent_grid(const MrtContext *ctx, uint32_t n) {
+    const uint32_t want = (n + 127) / 128;
+    const uint32_t cap = (uint32_t)ctx->sm_count * 8u;
+    return (int)(want < cap ? (want ? want : 1) : cap);
+}
+
 int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits) {
     MrtContext *ctx = s->ctx;
+    if (s->opts.accelerator == MRT_ACCEL_BVH && s->opts.bvh_mode == MRT_BVH_FAST) {
+        cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), ctx->stream);
+        TraceWork<false> w{d_rays, d_hits, nullptr, nullptr, n, ctx->d_counters};
+        k_trace_persistent<false><<<persistent_grid(ctx, n), 128, 0, ctx->stream>>>(s->dev, w);
+        return cuda_status(ctx, cudaGetLastError(), "k_trace_persistent");
+    }
     MRT_DISPATCH(launch_closest, s->opts.accelerator, s->opts.bvh_mode, s->dev, d_rays, n, d_hits, grid_for(ctx, n), ctx->stream);
     return cuda_status(ctx, cudaGetLastError(), "k_trace_closest");
 }
@@ -100,8 +148,11 @@ int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uin
 
 int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris) {
     MrtContext *ctx = s->ctx;
-    k_trace_counts<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(s->dev, d_rays, n, d_nodes, d_tris);
-    return cuda_status(ctx, cudaGetLastError(), "k_trace_counts");
+    // the same persistent traversal as the render and trace kernels, counting its fetches
+    cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), ctx->stream);
+    TraceWork<true> w{d_rays, nullptr, d_nodes, d_tris, n, ctx->d_counters};
+    k_trace_persistent<true><<<persistent_grid(ctx, n), 128, 0, ctx->stream>>>(s->dev, w);
+    return cuda_status(ctx, cudaGetLastError(), "k_trace_persistent<count>");
 }
 
 }  // namespace mrt_host

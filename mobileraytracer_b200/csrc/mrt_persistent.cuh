@@ -1,0 +1,200 @@
+// mrt_persistent.cuh - persistent closest-hit engine for the FAST BVH.
+//
+// Rays in a warp need very different amounts of work (a camera ray that misses the scene ends at
+// the root box, one that crosses a dense soup visits ~60 node pairs), so a one-ray-per-thread
+// kernel leaves most lanes idle behind the warp's longest ray.  Here every lane carries a
+// resumable traversal state and the warp loops:
+//   1. refill: lanes whose work item is finished take new items from a global counter, one
+//      atomicAdd per warp for all of them (ballot + popc);
+//   2. node phase: lanes that have no pending leaf visit node pairs until every lane has found a
+//      leaf or finished (warp vote), so node visits of different lanes run together;
+//   3. leaf phase: pending leaves are intersected together;
+//   4. completion: finished rays hand their result to the work item, which may start its next
+//      ray in the same lane (e.g. the next sample of a pixel).
+// Semantics are those of fast_trace(): the result is the lexicographic minimum (t, index) of the
+// triangles passing the reference test below the incoming length.
+#pragma once
+
+#include "mrt_trace.cuh"
+
+namespace mrt {
+
+constexpr uint32_t kPairNone = 0xFFFFFFFFu;
+
+struct FastTrav {
+    FastRay f;
+    float best_t;
+    uint32_t best_i;
+    uint32_t pair;          // child pair to expand next (kPairNone: pop the stack)
+    uint32_t leaf_first[2];
+    uint32_t leaf_count[2];
+    int n_leaf;
+    int sp;
+    bool have;
+    uint32_t c_nodes, c_tris;
+    uint32_t stack_n[kFastStack];
+    float stack_t[kFastStack];
+};
+
+template <bool kCount>
+__device__ __forceinline__ void trav_begin(const DevScene &s, const Ray &r, float len0, FastTrav &t) {
+    t.f = fast_ray(r);
+    t.best_t = len0;
+    t.best_i = 0;
+    t.have = false;
+    t.pair = kPairNone;
+    t.n_leaf = 0;
+    t.sp = 0;
+    t.c_nodes = 0;
+    t.c_tris = 0;
+    if (s.n_tri == 0) return;
+    const float4 lo = __ldg(&s.fnodes[0]), hi = __ldg(&s.fnodes[1]);
+    if (kCount) t.c_nodes++;
+    float tn;
+    if (!fast_slab(lo, hi, t.f, t.best_t, tn)) return;
+    const int b = __float_as_int(hi.w);
+    if (b > 0) {
+        t.leaf_first[0] = (uint32_t)__float_as_int(lo.w);
+        t.leaf_count[0] = (uint32_t)b;
+        t.n_leaf = 1;
+    } else {
+        t.pair = (uint32_t)__float_as_int(lo.w);
+    }
+}
+
+__device__ __forceinline__ bool trav_wants_node(const FastTrav &t) {
+    return t.n_leaf == 0 && (t.pair != kPairNone || t.sp > 0);
+}
+__device__ __forceinline__ bool trav_finished(const FastTrav &t) {
+    return t.n_leaf == 0 && t.pair == kPairNone && t.sp == 0;
+}
+
+// one node step: pop (with distance culling) or expand the current pair
+template <bool kCount>
+__device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t) {
+    if (t.pair == kPairNone) {
+        while (t.sp > 0) {
+            --t.sp;
+            if (t.stack_t[t.sp] <= t.best_t * 1.000001f) { t.pair = t.stack_n[t.sp]; break; }
+        }
+        return;
+    }
+    const uint32_t pair = t.pair;
+    if (pair + 1 >= s.n_fnodes) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
+    const float4 *p = s.fnodes + 2 * pair;
+    const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
+    if (kCount) t.c_nodes += 2;
+    float tl, tr;
+    const bool hl = fast_slab(l0, l1, t.f, t.best_t, tl);
+    const bool hr = fast_slab(r0, r1, t.f, t.best_t, tr);
+    const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
+    // leaves first, nearer one first
+    const bool ll = hl && lb > 0, rl = hr && rb > 0;
+    if (ll && rl && tr < tl) {
+        t.leaf_first[0] = (uint32_t)__float_as_int(r0.w); t.leaf_count[0] = (uint32_t)rb;
+        t.leaf_first[1] = (uint32_t)__float_as_int(l0.w); t.leaf_count[1] = (uint32_t)lb;
+        t.n_leaf = 2;
+    } else {
+        int k = 0;
+        if (ll) { t.leaf_first[k] = (uint32_t)__float_as_int(l0.w); t.leaf_count[k] = (uint32_t)lb; ++k; }
+        if (rl) { t.leaf_first[k] = (uint32_t)__float_as_int(r0.w); t.leaf_count[k] = (uint32_t)rb; ++k; }
+        t.n_leaf = k;
+    }
+    const bool il = hl && lb == 0, ir = hr && rb == 0;
+    if (il && ir) {
+        const bool left_first = tl <= tr;
+        if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
+        t.stack_n[t.sp] = (uint32_t)__float_as_int(left_first ? r0.w : l0.w);
+        t.stack_t[t.sp] = left_first ? tr : tl;
+        ++t.sp;
+        t.pair = (uint32_t)__float_as_int(left_first ? l0.w : r0.w);
+    } else if (il) {
+        t.pair = (uint32_t)__float_as_int(l0.w);
+    } else if (ir) {
+        t.pair = (uint32_t)__float_as_int(r0.w);
+    } else {
+        t.pair = kPairNone;
+    }
+}
+
+template <bool kCount>
+__device__ __forceinline__ void trav_leaf_step(const DevScene &s, const Ray &r, FastTrav &t) {
+    FastCounts cnt{0, 0};
+    for (int k = 0; k < t.n_leaf; ++k)
+        fast_leaf<kCount>(s, r, t.leaf_first[k], t.leaf_count[k], t.best_t, t.best_i, t.have, cnt);
+    if (kCount) t.c_tris += cnt.tris;
+    t.n_leaf = 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// the persistent loop.  Work provides:
+//   uint32_t total() const; uint32_t *counter() const;
+//   bool begin(uint32_t item, Lane &lane, Ray &r)     -> false: nothing to trace for this item
+//   bool finish(Lane &lane, Ray &r, bool hit, float t, uint32_t id, const FastTrav &tr)
+//        -> true: r holds the item's next ray (same lane continues)
+// Planes and spheres are tested in order before the tree and area lights after it
+// (Shader.cpp:124-150), all with the reference accept rule.
+// ---------------------------------------------------------------------------------------------
+template <bool kCount, class Work, class Lane>
+__device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastTrav &t, float &len, uint32_t &id) {
+    len = kRayLengthMax;
+    id = MRT_HIT_NONE;
+    naive_trace<kPlane>(s, r, len, id);
+    naive_trace<kSphere>(s, r, len, id);
+    trav_begin<kCount>(s, r, len, t);
+}
+
+template <bool kCount, class Work, class Lane>
+__device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const int lane_id = threadIdx.x & 31;
+    const uint32_t total = work.total();
+    bool active = false;
+    bool exhausted = false;
+    Ray r;
+    FastTrav t;
+    float len0 = kRayLengthMax;   // distance after planes and spheres
+    uint32_t id0 = MRT_HIT_NONE;
+    for (;;) {
+        // 1. refill idle lanes (one atomic per warp)
+        const uint32_t idle = __ballot_sync(FULL, !active);
+        if (!exhausted && (__popc(idle) >= 8 || idle == FULL)) {
+            const int leader = __ffs(idle) - 1;
+            uint32_t base = 0;
+            if (lane_id == leader) base = atomicAdd(work.counter(), (uint32_t)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
+            if (!active) {
+                const uint32_t item = base + __popc(idle & ((1u << lane_id) - 1u));
+                if (item < total && work.begin(item, lane, r)) {
+                    start_ray<kCount, Work, Lane>(s, r, t, len0, id0);
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        // 2. node phase
+        for (;;) {
+            const bool w = active && trav_wants_node(t);
+            if (!__any_sync(FULL, w)) break;
+            if (w) trav_node_step<kCount>(s, t);
+        }
+        // 3. leaf phase
+        if (active && t.n_leaf > 0) trav_leaf_step<kCount>(s, r, t);
+        // 4. completion
+        if (active && trav_finished(t)) {
+            float len = len0;
+            uint32_t id = id0;
+            if (t.have) { len = t.best_t; id = hid(MRT_PRIM_TRIANGLE, t.best_i); }
+            const bool hit_light = lights_trace(s, r, len, id);
+            const bool hit = id != MRT_HIT_NONE || hit_light;
+            if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(s, r, t, len0, id0);
+            else active = false;
+        }
+    }
+}
+
+}  // namespace mrt

@@ -22,7 +22,7 @@
 #include <cstring>
 
 #include "mrt_internal.h"
-#include "mrt_trace.cuh"
+#include "mrt_persistent.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
@@ -148,6 +148,75 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
         p.bitmap[k.index] = bm;
         if (slot >= 0) p.accum[slot] = acc;
     }
+}
+
+// persistent FAST-BVH NoShadows: work item = pixel task; the lane traces the pixel's samples in
+// order and keeps its running mean in registers.  Implicit tasks are fetched in 8x4-pixel tiles
+// (when the image allows) so the rays of a warp start coherent.
+struct NsLane {
+    Task k;
+    uint32_t pixel;
+    int64_t slot;
+    uint32_t bm;
+    float4 acc;
+    uint32_t si;
+};
+
+struct NsWork {
+    const DevScene *s;
+    const RenderParams *p;
+    uint32_t first, count;
+    uint32_t *ctr;
+    uint32_t tiles_x;   // 0: row-major tasks
+    __device__ uint32_t total() const { return count; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ Ray ray_for(const NsLane &lane) const {
+        const Stream st = make_stream(p->seed, lane.pixel, p->spp_offset + lane.si, p->strata, p->constant_value);
+        return primary_ray(*p, lane.k, st);
+    }
+    __device__ bool begin(uint32_t item, NsLane &lane, Ray &r) const {
+        uint32_t t = first + item;
+        if (tiles_x) {
+            const uint32_t tile = item >> 5, w = item & 31u;
+            const uint32_t x = (tile % tiles_x) * 8u + (w & 7u), y = (tile / tiles_x) * 4u + (w >> 3);
+            t = y * p->width + x;
+        }
+        lane.k = task_of(*p, t);
+        lane.pixel = lane.k.y * p->width + lane.k.x;
+        lane.slot = p->accum ? accum_slot(*p, lane.k) : -1;
+        lane.bm = p->bitmap[lane.k.index];
+        lane.acc = lane.slot >= 0 ? p->accum[lane.slot] : make_float4(0, 0, 0, 0);
+        lane.si = 0;
+        r = ray_for(lane);
+        return true;
+    }
+    __device__ bool finish(NsLane &lane, Ray &r, bool hit, float, uint32_t id, const FastTrav &) const {
+        const uint32_t sample = p->spp_offset + lane.si;
+        V3 rgb{0.0f, 0.0f, 0.0f};
+        if (hit) {
+            Isect it;
+            if (make_isect(*s, r, id, it)) {
+                const Stream st = make_stream(p->seed, lane.pixel, sample, p->strata, p->constant_value);
+                rgb = shade_noshadows(*s, *p, st, it, 1u);
+            }
+        }
+        lane.bm = incremental_avg(rgb, lane.bm, sample + 1u);
+        lane.acc.x += rgb.x; lane.acc.y += rgb.y; lane.acc.z += rgb.z; lane.acc.w += 1.0f;
+        if (++lane.si < p->spp) {
+            r = ray_for(lane);
+            return true;
+        }
+        p->bitmap[lane.k.index] = lane.bm;
+        if (lane.slot >= 0) p->accum[lane.slot] = lane.acc;
+        return false;
+    }
+};
+
+__global__ void __launch_bounds__(128) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
+                                                               uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
+    NsWork w{&s, &p, first, count, ctr, tiles_x};
+    NsLane lane;
+    persistent_closest<false>(s, w, lane);
 }
 
 // ============================== wavefront ====================================================
@@ -709,9 +778,18 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     s->progress.store(0);
     cudaEventRecord(ctx->ev0, q);
     if (o->shader == MRT_SHADER_NOSHADOWS) {
+        const bool fast = accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST;
+        const uint32_t rows = 16u * (o->height / 16u);
+        const uint32_t tiles_x = (plan.implicit && o->width % 8u == 0 && rows % 4u == 0) ? o->width / 8u : 0u;
         for (size_t r = 0; r < plan.round_first.size(); ++r) {
             if (s->stop.load()) return MRT_ERR_CANCELLED;
-            MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, plan.round_first[r], plan.round_count[r], grid, q);
+            if (fast) {
+                cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
+                k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
+                                                                         plan.round_count[r], ctx->d_counters, tiles_x);
+            } else {
+                MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, plan.round_first[r], plan.round_count[r], grid, q);
+            }
         }
         rays_closest = (uint64_t)plan.n_tasks * o->spp;
     } else {
