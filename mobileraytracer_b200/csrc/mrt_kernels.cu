@@ -89,6 +89,28 @@ struct TraceWork {
     }
 };
 
+struct AnyWork {
+    const MrtRay *rays;
+    const float *dist;
+    uint8_t *occ;
+    uint32_t n;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return n; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ bool begin(uint32_t item, TraceLane &lane, Ray &r, float &d) const {
+        lane.i = item;
+        r = load_ray(rays, item);
+        d = dist[item];
+        return true;
+    }
+    __device__ void finish(TraceLane &lane, bool occluded) const { occ[lane.i] = occluded ? 1 : 0; }
+};
+
+__global__ void __launch_bounds__(128) k_trace_any_persistent(DevScene s, AnyWork work) {
+    TraceLane lane;
+    persistent_any(s, work, lane);
+}
+
 template <bool kCount>
 __global__ void __launch_bounds__(128) k_trace_persistent(DevScene s, TraceWork<kCount> work) {
     TraceLane lane;
@@ -142,6 +164,12 @@ int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *
 
 int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uint32_t n, uint8_t *d_occ) {
     MrtContext *ctx = s->ctx;
+    if (s->opts.accelerator == MRT_ACCEL_BVH && s->opts.bvh_mode == MRT_BVH_FAST) {
+        cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), ctx->stream);
+        AnyWork w{d_rays, d_dist, d_occ, n, ctx->d_counters};
+        k_trace_any_persistent<<<persistent_grid(ctx, n), 128, 0, ctx->stream>>>(s->dev, w);
+        return cuda_status(ctx, cudaGetLastError(), "k_trace_any_persistent");
+    }
     MRT_DISPATCH(launch_any, s->opts.accelerator, s->opts.bvh_mode, s->dev, d_rays, d_dist, n, d_occ, grid_for(ctx, n), ctx->stream);
     return cuda_status(ctx, cudaGetLastError(), "k_trace_any");
 }

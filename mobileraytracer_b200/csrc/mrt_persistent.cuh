@@ -26,14 +26,17 @@ struct FastTrav {
     float best_t;
     uint32_t best_i;
     uint32_t pair;          // child pair to expand next (kPairNone: pop the stack)
-    uint32_t leaf_first[2];
-    uint32_t leaf_count[2];
+    uint32_t leaf0_first, leaf0_count, leaf1_first, leaf1_count;   // pending leaves (named: stay in registers)
     int n_leaf;
     int sp;
     bool have;
     uint32_t c_nodes, c_tris;
-    uint32_t stack_n[kFastStack];
-    float stack_t[kFastStack];
+};
+
+// the traversal stack lives apart from the scalar state so the scalars stay in registers
+struct TravStack {
+    uint32_t n[kFastStack];
+    float t[kFastStack];
 };
 
 template <bool kCount>
@@ -54,8 +57,8 @@ __device__ __forceinline__ void trav_begin(const DevScene &s, const Ray &r, floa
     if (!fast_slab(lo, hi, t.f, t.best_t, tn)) return;
     const int b = __float_as_int(hi.w);
     if (b > 0) {
-        t.leaf_first[0] = (uint32_t)__float_as_int(lo.w);
-        t.leaf_count[0] = (uint32_t)b;
+        t.leaf0_first = (uint32_t)__float_as_int(lo.w);
+        t.leaf0_count = (uint32_t)b;
         t.n_leaf = 1;
     } else {
         t.pair = (uint32_t)__float_as_int(lo.w);
@@ -71,11 +74,11 @@ __device__ __forceinline__ bool trav_finished(const FastTrav &t) {
 
 // one node step: pop (with distance culling) or expand the current pair
 template <bool kCount>
-__device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t) {
+__device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t, TravStack &st) {
     if (t.pair == kPairNone) {
         while (t.sp > 0) {
             --t.sp;
-            if (t.stack_t[t.sp] <= t.best_t * 1.000001f) { t.pair = t.stack_n[t.sp]; break; }
+            if (st.t[t.sp] <= t.best_t * 1.000001f) { t.pair = st.n[t.sp]; break; }
         }
         return;
     }
@@ -90,22 +93,24 @@ __device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t) {
     const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
     // leaves first, nearer one first
     const bool ll = hl && lb > 0, rl = hr && rb > 0;
-    if (ll && rl && tr < tl) {
-        t.leaf_first[0] = (uint32_t)__float_as_int(r0.w); t.leaf_count[0] = (uint32_t)rb;
-        t.leaf_first[1] = (uint32_t)__float_as_int(l0.w); t.leaf_count[1] = (uint32_t)lb;
+    const bool swap = ll && rl && tr < tl;
+    const uint32_t lf = (uint32_t)__float_as_int(l0.w), rf = (uint32_t)__float_as_int(r0.w);
+    if (ll && rl) {
+        t.leaf0_first = swap ? rf : lf; t.leaf0_count = (uint32_t)(swap ? rb : lb);
+        t.leaf1_first = swap ? lf : rf; t.leaf1_count = (uint32_t)(swap ? lb : rb);
         t.n_leaf = 2;
+    } else if (ll || rl) {
+        t.leaf0_first = ll ? lf : rf; t.leaf0_count = (uint32_t)(ll ? lb : rb);
+        t.n_leaf = 1;
     } else {
-        int k = 0;
-        if (ll) { t.leaf_first[k] = (uint32_t)__float_as_int(l0.w); t.leaf_count[k] = (uint32_t)lb; ++k; }
-        if (rl) { t.leaf_first[k] = (uint32_t)__float_as_int(r0.w); t.leaf_count[k] = (uint32_t)rb; ++k; }
-        t.n_leaf = k;
+        t.n_leaf = 0;
     }
     const bool il = hl && lb == 0, ir = hr && rb == 0;
     if (il && ir) {
         const bool left_first = tl <= tr;
         if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
-        t.stack_n[t.sp] = (uint32_t)__float_as_int(left_first ? r0.w : l0.w);
-        t.stack_t[t.sp] = left_first ? tr : tl;
+        st.n[t.sp] = (uint32_t)__float_as_int(left_first ? r0.w : l0.w);
+        st.t[t.sp] = left_first ? tr : tl;
         ++t.sp;
         t.pair = (uint32_t)__float_as_int(left_first ? l0.w : r0.w);
     } else if (il) {
@@ -120,8 +125,8 @@ __device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t) {
 template <bool kCount>
 __device__ __forceinline__ void trav_leaf_step(const DevScene &s, const Ray &r, FastTrav &t) {
     FastCounts cnt{0, 0};
-    for (int k = 0; k < t.n_leaf; ++k)
-        fast_leaf<kCount>(s, r, t.leaf_first[k], t.leaf_count[k], t.best_t, t.best_i, t.have, cnt);
+    fast_leaf<kCount>(s, r, t.leaf0_first, t.leaf0_count, t.best_t, t.best_i, t.have, cnt);
+    if (t.n_leaf > 1) fast_leaf<kCount>(s, r, t.leaf1_first, t.leaf1_count, t.best_t, t.best_i, t.have, cnt);
     if (kCount) t.c_tris += cnt.tris;
     t.n_leaf = 0;
 }
@@ -153,6 +158,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
     bool exhausted = false;
     Ray r;
     FastTrav t;
+    TravStack stk;
     float len0 = kRayLengthMax;   // distance after planes and spheres
     uint32_t id0 = MRT_HIT_NONE;
     for (;;) {
@@ -180,7 +186,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
         for (;;) {
             const bool w = active && trav_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) trav_node_step<kCount>(s, t);
+            if (w) trav_node_step<kCount>(s, t, stk);
         }
         // 3. leaf phase
         if (active && t.n_leaf > 0) trav_leaf_step<kCount>(s, r, t);
@@ -193,6 +199,150 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             const bool hit = id != MRT_HIT_NONE || hit_light;
             if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(s, r, t, len0, id0);
             else active = false;
+        }
+    }
+}
+
+}  // namespace mrt
+
+namespace mrt {
+
+// ---------------------------------------------------------------------------------------------
+// any-hit (Shader::shadowTrace, Shader.cpp:162-187): planes and spheres in order, then the tree;
+// the first occluder ends the ray, so no ordering and no distance culling beyond `dist`.
+// Work provides total(), counter(), begin(item, lane, r, dist) and finish(lane, occluded).
+// ---------------------------------------------------------------------------------------------
+struct OccTrav {
+    FastRay f;
+    float dist;
+    uint32_t pair;
+    uint32_t leaf0_first, leaf0_count, leaf1_first, leaf1_count;
+    int n_leaf;
+    int sp;
+    bool occluded;
+};
+
+__device__ __forceinline__ void occ_begin(const DevScene &s, const Ray &r, float dist, OccTrav &t) {
+    t.dist = dist;
+    t.pair = kPairNone;
+    t.n_leaf = 0;
+    t.sp = 0;
+    t.occluded = naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist);
+    if (t.occluded || s.n_tri == 0) return;
+    t.f = fast_ray(r);
+    const float4 lo = __ldg(&s.fnodes[0]), hi = __ldg(&s.fnodes[1]);
+    float tn;
+    if (!fast_slab(lo, hi, t.f, dist, tn)) return;
+    const int b = __float_as_int(hi.w);
+    if (b > 0) {
+        t.leaf0_first = (uint32_t)__float_as_int(lo.w);
+        t.leaf0_count = (uint32_t)b;
+        t.n_leaf = 1;
+    } else {
+        t.pair = (uint32_t)__float_as_int(lo.w);
+    }
+}
+
+__device__ __forceinline__ bool occ_wants_node(const OccTrav &t) {
+    return !t.occluded && t.n_leaf == 0 && (t.pair != kPairNone || t.sp > 0);
+}
+__device__ __forceinline__ bool occ_finished(const OccTrav &t) {
+    return t.occluded || (t.n_leaf == 0 && t.pair == kPairNone && t.sp == 0);
+}
+
+__device__ __forceinline__ void occ_node_step(const DevScene &s, OccTrav &t, uint32_t *stack_n) {
+    if (t.pair == kPairNone) {
+        if (t.sp > 0) t.pair = stack_n[--t.sp];
+        return;
+    }
+    const uint32_t pair = t.pair;
+    if (pair + 1 >= s.n_fnodes) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
+    const float4 *p = s.fnodes + 2 * pair;
+    const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
+    float tl, tr;
+    const bool hl = fast_slab(l0, l1, t.f, t.dist, tl);
+    const bool hr = fast_slab(r0, r1, t.f, t.dist, tr);
+    const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
+    const bool ll = hl && lb > 0, rl = hr && rb > 0;
+    const uint32_t lf = (uint32_t)__float_as_int(l0.w), rf = (uint32_t)__float_as_int(r0.w);
+    if (ll && rl) {
+        t.leaf0_first = lf; t.leaf0_count = (uint32_t)lb; t.leaf1_first = rf; t.leaf1_count = (uint32_t)rb;
+        t.n_leaf = 2;
+    } else if (ll || rl) {
+        t.leaf0_first = ll ? lf : rf; t.leaf0_count = (uint32_t)(ll ? lb : rb);
+        t.n_leaf = 1;
+    } else {
+        t.n_leaf = 0;
+    }
+    const bool il = hl && lb == 0, ir = hr && rb == 0;
+    if (il && ir) {
+        if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
+        stack_n[t.sp++] = (uint32_t)__float_as_int(r0.w);
+        t.pair = (uint32_t)__float_as_int(l0.w);
+    } else if (il) {
+        t.pair = (uint32_t)__float_as_int(l0.w);
+    } else if (ir) {
+        t.pair = (uint32_t)__float_as_int(r0.w);
+    } else {
+        t.pair = kPairNone;
+    }
+}
+
+__device__ __forceinline__ void occ_leaf_step(const DevScene &s, const Ray &r, OccTrav &t) {
+    for (int q = 0; q < t.n_leaf && !t.occluded; ++q) {
+        const uint32_t first = q == 0 ? t.leaf0_first : t.leaf1_first, count = q == 0 ? t.leaf0_count : t.leaf1_count;
+        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4 A = __ldg(&s.ftris[3 * k]);
+            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
+            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
+            if (tri_occ(v3(A), v3(AB), v3(AC), r, t.dist)) { t.occluded = true; break; }
+        }
+    }
+    t.n_leaf = 0;
+}
+
+template <class Work, class Lane>
+__device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const int lane_id = threadIdx.x & 31;
+    const uint32_t total = work.total();
+    bool active = false;
+    bool exhausted = false;
+    Ray r;
+    OccTrav t;
+    uint32_t stack_n[kFastStack];
+    for (;;) {
+        const uint32_t idle = __ballot_sync(FULL, !active);
+        if (!exhausted && (__popc(idle) >= 8 || idle == FULL)) {
+            const int leader = __ffs(idle) - 1;
+            uint32_t base = 0;
+            if (lane_id == leader) base = atomicAdd(work.counter(), (uint32_t)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
+            if (!active) {
+                const uint32_t item = base + __popc(idle & ((1u << lane_id) - 1u));
+                float dist;
+                if (item < total && work.begin(item, lane, r, dist)) {
+                    occ_begin(s, r, dist, t);
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        for (;;) {
+            const bool w = active && occ_wants_node(t);
+            if (!__any_sync(FULL, w)) break;
+            if (w) occ_node_step(s, t, stack_n);
+        }
+        if (active && t.n_leaf > 0) occ_leaf_step(s, r, t);
+        if (active && occ_finished(t)) {
+            work.finish(lane, t.occluded);
+            active = false;
         }
     }
 }

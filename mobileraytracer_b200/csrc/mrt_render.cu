@@ -515,6 +515,67 @@ __global__ void __launch_bounds__(128) k_wave_shadow(DevScene s, WaveState w, in
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[1], (unsigned long long)n);
 }
 
+// persistent FAST-BVH versions of extend and shadow (work items: the level's rays / shadow rays)
+struct WaveLane {
+    uint32_t idx;
+};
+struct ExtendWork {
+    WaveState w;
+    Level L;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return L.count; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ bool begin(uint32_t item, WaveLane &lane, Ray &r) const {
+        lane.idx = L.start + item;
+        r = ray_of(w.rays[lane.idx]);
+        return true;
+    }
+    __device__ bool finish(WaveLane &lane, Ray &, bool hit, float t, uint32_t id, const FastTrav &) const {
+        w.nodes[lane.idx].hit_t = t;
+        w.nodes[lane.idx].hit_id = hit ? id : MRT_HIT_NONE;
+        return false;
+    }
+};
+struct ShadowWork {
+    WaveState w;
+    uint32_t n;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return n; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ bool begin(uint32_t item, WaveLane &lane, Ray &r, float &dist) const {
+        const ShadowRec sr = w.shadows[item];
+        lane.idx = item;
+        r.o = V3{sr.ox, sr.oy, sr.oz};
+        r.d = V3{sr.dx, sr.dy, sr.dz};
+        r.depth = 0;
+        r.exclude = sr.exclude;
+        dist = sr.dist;
+        return true;
+    }
+    __device__ void finish(WaveLane &lane, bool occluded) const {
+        if (occluded) {
+            const ShadowRec &sr = w.shadows[lane.idx];
+            atomicOr(&w.nodes[sr.node].occluded, 1u << (sr.j & 31u));
+        }
+    }
+};
+
+__global__ void __launch_bounds__(128) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+    const Level L = clamp_level(w, w.levels[level]);
+    ExtendWork work{w, L, ctr};
+    WaveLane lane;
+    persistent_closest<false>(s, work, lane);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
+}
+
+__global__ void __launch_bounds__(128) k_wave_shadow_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+    const uint32_t n = min(w.levels[level].shadow_count, w.shadow_cap);
+    ShadowWork work{w, n, ctr};
+    WaveLane lane;
+    persistent_any(s, work, lane);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[1], (unsigned long long)n);
+}
+
 // bottom-up evaluation of one level: the shade() bodies after their recursive calls return
 __global__ void __launch_bounds__(128) k_wave_resolve(DevScene s, RenderParams p, WaveState w, int level) {
     const Level L = clamp_level(w, w.levels[level]);
@@ -689,7 +750,15 @@ void launch_noshadows(const DevScene &s, const RenderParams &p, uint32_t first, 
 }
 
 template <int ACCEL, int MODE>
-void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState &w, int level, int grid, cudaStream_t q) {
+void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState &w, int level, int grid, cudaStream_t q,
+                       uint32_t *ctrs) {
+    if (ACCEL == MRT_ACCEL_BVH && MODE == MRT_BVH_FAST) {
+        // counters [2 * level] and [2 * level + 1] were zeroed for this wave
+        k_wave_extend_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
+        k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
+        k_wave_shadow_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level + 1);
+        return;
+    }
     k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
     k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
     k_wave_shadow<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
@@ -801,6 +870,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         const uint64_t ray_cap = (uint64_t)wave * (uint64_t)(levels + 2);
         const uint64_t shadow_cap = (uint64_t)wave * std::max(1u, o->spl) * 2ull;
         if (ray_cap > 0xFFFFFFF0ull) { set_error(ctx, "mrt_render: wave too large"); return MRT_ERR_ARG; }
+        if (2 * (levels + 1) > 64) { set_error(ctx, "mrt_render: depth_max above 30"); return MRT_ERR_ARG; }
         if (st == MRT_OK) st = ensure(ctx, s->work[1], sizeof(RayRec) * ray_cap);
         if (st == MRT_OK) st = ensure(ctx, s->work[2], sizeof(NodeRec) * ray_cap);
         if (st == MRT_OK) st = ensure(ctx, s->work[3], sizeof(ShadowRec) * shadow_cap);
@@ -826,8 +896,10 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 w.root_first = (uint32_t)r0;
                 w.n_roots = (uint32_t)std::min<uint64_t>(wave, total_roots - r0);
                 cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
+                cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
                 k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
-                for (int b = 0; b < levels; ++b) MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q);
+                for (int b = 0; b < levels; ++b)
+                    MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);
                 for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
                 k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
                 s->progress.store((uint32_t)((r0 + w.n_roots) / std::max<uint64_t>(1, plan.round_count[rd])));
