@@ -230,6 +230,17 @@ int mrt_trace_closest_counts(MrtScene *scene, const MrtRay *rays, uint32_t n, ui
 int mrt_render(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *opts,
                uint32_t *bitmap, uint32_t stride_bytes, float *accum, uint32_t mem,
                MrtRenderStats *stats);
+/* mrt_render without any device allocation (no counterpart in the reference).  For callers that
+ * cannot allocate device memory while rendering: code inside a CUDA stream capture, processes whose
+ * device memory belongs to another allocator or a fixed budget, latency-critical threads.  bitmap
+ * and accum are device pointers; all other scratch is one static device array of 12 MiB at most that
+ * every GPU loading the library keeps until exit.  Supports the plain-rectangle block schedule only
+ * (width a multiple of 16, stride_bytes = 4 * width, height / (height / 16) == 16), samplesLight <= 4
+ * and depth_max <= 10; anything larger returns MRT_ERR_ARG.  The first call on a device looks up the
+ * array's address (make it before any stream capture).  Calls share the array: calls that overlap
+ * on the GPU race. */
+int mrt_render_noalloc(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *opts, uint32_t *bitmap,
+                       uint32_t stride_bytes, float *accum, MrtRenderStats *stats);
 void mrt_render_stop(MrtScene *scene);
 uint32_t mrt_render_progress(const MrtScene *scene);
 

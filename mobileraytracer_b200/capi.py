@@ -142,6 +142,8 @@ def load() -> ctypes.CDLL:
         "mrt_trace_closest_counts": (ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32]),
         "mrt_render": (ctypes.c_int, [vp, P(MrtCamera), P(MrtRenderOpts), vp, ctypes.c_uint32, vp, ctypes.c_uint32,
                                       P(MrtRenderStats)]),
+        "mrt_render_noalloc": (ctypes.c_int, [vp, P(MrtCamera), P(MrtRenderOpts), vp, ctypes.c_uint32, vp,
+                                              P(MrtRenderStats)]),
         "mrt_render_stop": (None, [vp]),
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
     }
@@ -157,5 +159,5 @@ EXPORTED_SYMBOLS = [
     "mrt_context_create", "mrt_context_destroy", "mrt_context_error", "mrt_context_synchronize",
     "mrt_context_stream", "mrt_scene_create", "mrt_scene_destroy", "mrt_scene_build", "mrt_scene_device_bytes",
     "mrt_scene_accel_info", "mrt_trace_closest", "mrt_trace_any", "mrt_trace_closest_counts", "mrt_render",
-    "mrt_render_stop", "mrt_render_progress",
+    "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress",
 ]

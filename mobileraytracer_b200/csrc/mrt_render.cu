@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 
 #include "mrt_internal.h"
 #include "mrt_persistent.cuh"
@@ -988,3 +989,170 @@ void mrt_render_stop(MrtScene *s) {
 uint32_t mrt_render_progress(const MrtScene *s) { return s ? s->progress.load() : 0u; }
 
 }  // extern "C"
+
+// =============================================================================================
+// mrt_render_noalloc: the same render with every piece of scratch in a fixed device array.
+//
+// For callers that cannot allocate device memory while they render: code running inside a
+// cudaStreamBeginCapture region (an allocation there would break the capture), a process whose
+// device memory is owned by another allocator or a fixed budget, or a latency-critical thread that
+// must not hit cudaMalloc's implicit synchronisation.  The caller passes device buffers for the
+// bitmap and the sums; everything else the kernels need (work counters, the wave's ray / node /
+// shadow queues, per-sample values) lives in g_noalloc_scratch below, which every GPU that loads
+// the library holds until the process exits.
+//
+// Limits of this variant: image sizes whose block schedule is the plain rectangle (width a multiple
+// of 16, row pitch = width, as the reference CLI sizes images), samplesLight <= kNoAllocMaxSpl,
+// depth_max <= kNoAllocMaxDepth; waves of kNoAllocWave camera paths.  Larger requests fail with
+// MRT_ERR_ARG.  The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
+// array: calls that overlap on the GPU (two host threads, or two contexts on one device) race.
+// =============================================================================================
+namespace {
+
+constexpr uint32_t kNoAllocWave = 4096;
+constexpr int kNoAllocMaxDepth = 10;
+constexpr uint32_t kNoAllocMaxSpl = 4;
+constexpr int kNoAllocLevels = kNoAllocMaxDepth + 1;
+constexpr size_t kNaCounters = 0;                                   // 64 x uint32 work counters
+constexpr size_t kNaWaveCounters = 256;                             // 2 x uint64 ray counters
+constexpr size_t kNaLevels = 512;                                   // Level x (levels + 2)
+constexpr size_t kNaRoot = 1024;                                    // float4 x wave
+constexpr size_t kNaRays = kNaRoot + 16ull * kNoAllocWave;
+constexpr size_t kNaRayCap = (size_t)kNoAllocWave * (kNoAllocLevels + 2);
+constexpr size_t kNaNodes = kNaRays + sizeof(RayRec) * kNaRayCap;
+constexpr size_t kNaShadows = kNaNodes + sizeof(NodeRec) * kNaRayCap;
+constexpr size_t kNaShadowCap = (size_t)kNoAllocWave * kNoAllocMaxSpl * 2;
+constexpr size_t kNoAllocScratchBytes = (kNaShadows + sizeof(ShadowRec) * kNaShadowCap + 255) & ~(size_t)255;
+static_assert(sizeof(Level) * (kNoAllocLevels + 2) <= kNaRoot - kNaLevels, "level table overlaps");
+static_assert(kNoAllocScratchBytes <= 12u * 1024u * 1024u, "scratch above 12 MiB");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// device address of g_noalloc_scratch per device (looked up once, with that device current)
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(MrtContext *ctx, unsigned char **out) {
+    if (ctx->device < 0 || ctx->device >= 64) { set_error(ctx, "mrt_render_noalloc: device index above 63"); return MRT_ERR_ARG; }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return cuda_status(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+        g_noalloc_ptr[ctx->device] = ptr;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_ptr[ctx->device]);
+    return MRT_OK;
+}
+
+}  // namespace
+
+extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *bitmap,
+                                  uint32_t stride_bytes, float *accum, MrtRenderStats *stats) {
+    if (!s || !cam || !o || !bitmap) return MRT_ERR_ARG;
+    MrtContext *ctx = s->ctx;
+    if (!s->built) { set_error(ctx, "mrt_render_noalloc before mrt_scene_build"); return MRT_ERR_STATE; }
+    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_PATHTRACER || o->spp == 0 || o->spl == 0 ||
+        o->width < 16 || o->height < 16 || cam->kind != MRT_CAMERA_PERSPECTIVE || o->pixel_sampler < 0 ||
+        o->pixel_sampler > 3 || o->light_sampler < 0 || o->light_sampler > 3 || o->rr_sampler < 0 || o->rr_sampler > 3) {
+        set_error(ctx, "mrt_render_noalloc: invalid options");
+        return MRT_ERR_ARG;
+    }
+    const uint32_t bsy = o->height / 16u;
+    if (o->width % 16u != 0 || stride_bytes != 4u * o->width || o->height / bsy != 16u) {
+        set_error(ctx, "mrt_render_noalloc: width must be a multiple of 16 with row pitch = width and height / (height / 16) == 16");
+        return MRT_ERR_ARG;
+    }
+    if (o->spl > kNoAllocMaxSpl || o->depth_max > kNoAllocMaxDepth || o->depth_max < 0) {
+        set_error(ctx, "mrt_render_noalloc: samplesLight <= %u and 0 <= depth_max <= %d in this variant", kNoAllocMaxSpl,
+                  kNoAllocMaxDepth);
+        return MRT_ERR_ARG;
+    }
+    if (((uintptr_t)bitmap & 3u) || ((uintptr_t)accum & 15u)) {
+        set_error(ctx, "mrt_render_noalloc: bitmap must be 4-byte aligned and the sums 16-byte aligned");
+        return MRT_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    unsigned char *scratch = nullptr;
+    int st = noalloc_scratch(ctx, &scratch);
+    if (st != MRT_OK) return st;
+    cudaStream_t q = ctx->stream;
+    s->stop.store(0);
+    RenderParams p{};
+    p.cam = make_camera(*cam);
+    p.width = o->width; p.height = o->height; p.spp = o->spp; p.spl = o->spl; p.stride_px = o->width;
+    p.pixel_sampler = o->pixel_sampler; p.light_sampler = o->light_sampler; p.rr_sampler = o->rr_sampler;
+    p.shader = o->shader; p.constant_value = o->constant_value;
+    p.depth_min = o->depth_min; p.depth_max = o->depth_max;
+    p.seed = o->seed; p.spp_offset = o->spp_offset;
+    p.strata = o->spp;
+    p.bitmap = bitmap;
+    p.accum = (float4 *)accum;
+    p.inv_w = 1.0f / (float)o->width;
+    p.inv_h = 1.0f / (float)o->height;
+    p.pw = 0.5f / (float)o->width;
+    p.ph = 0.5f / (float)o->height;
+    p.tasks = nullptr;
+    p.n_tasks = o->width * 16u * bsy;
+    uint32_t *counters = reinterpret_cast<uint32_t *>(scratch + kNaCounters);
+    const int accel = s->opts.accelerator, mode = s->opts.bvh_mode;
+    const int grid = ctx->sm_count * 16;
+    uint64_t rays_closest = 0, rays_shadow = 0;
+    s->progress.store(0);
+    cudaEventRecord(ctx->ev0, q);
+    if (o->shader == MRT_SHADER_NOSHADOWS) {
+        if (accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST) {
+            const uint32_t tiles_x = ((16u * bsy) % 4u == 0) ? o->width / 8u : 0u;
+            cudaMemsetAsync(counters, 0, sizeof(uint32_t), q);
+            k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, 0u, p.n_tasks, counters, tiles_x);
+        } else {
+            MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, 0u, p.n_tasks, grid, q);
+        }
+        rays_closest = (uint64_t)p.n_tasks * o->spp;
+    } else {
+        const int levels = std::max(1, o->depth_max + 1);
+        WaveState w{};
+        w.rays = reinterpret_cast<RayRec *>(scratch + kNaRays);
+        w.nodes = reinterpret_cast<NodeRec *>(scratch + kNaNodes);
+        w.shadows = reinterpret_cast<ShadowRec *>(scratch + kNaShadows);
+        w.levels = reinterpret_cast<Level *>(scratch + kNaLevels);
+        w.root_rgb = reinterpret_cast<float4 *>(scratch + kNaRoot);
+        w.counters = reinterpret_cast<unsigned long long *>(scratch + kNaWaveCounters);
+        w.ray_cap = (uint32_t)std::min<size_t>(kNaRayCap, (size_t)kNoAllocWave * (levels + 2));
+        w.shadow_cap = (uint32_t)std::min<size_t>(kNaShadowCap, (size_t)kNoAllocWave * o->spl * 2);
+        cudaMemsetAsync(w.counters, 0, 16, q);
+        const uint64_t total_roots = (uint64_t)p.n_tasks * o->spp;
+        p.task_base = 0;
+        for (uint64_t r0 = 0; r0 < total_roots; r0 += kNoAllocWave) {
+            if (s->stop.load()) return MRT_ERR_CANCELLED;
+            w.root_first = (uint32_t)r0;
+            w.n_roots = (uint32_t)std::min<uint64_t>(kNoAllocWave, total_roots - r0);
+            cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
+            cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
+            k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
+            for (int b = 0; b < levels; ++b) MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, counters);
+            for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
+            k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
+        }
+        unsigned long long cnt[2] = {0, 0};
+        st = cuda_status(ctx, cudaMemcpyAsync(cnt, w.counters, 16, cudaMemcpyDeviceToHost, q), "counters");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "render");
+        rays_closest = cnt[0];
+        rays_shadow = cnt[1];
+    }
+    cudaEventRecord(ctx->ev1, q);
+    if (st == MRT_OK) st = cuda_status(ctx, cudaGetLastError(), "render kernels");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaEventSynchronize(ctx->ev1), "render");
+    if (st == MRT_OK) st = check_kernel_error(ctx);
+    s->progress.store(o->spp);
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->rays_closest = rays_closest;
+        stats->rays_shadow = rays_shadow;
+        stats->paths = (uint64_t)p.n_tasks * o->spp;
+        stats->device_ms = ms;
+    }
+    return st;
+}
