@@ -215,19 +215,163 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+BATCH_WORKLOAD = ("config 4: 256 PathTracer jobs (depth 6, Russian roulette beyond depth 3, 1 light sample), "
+                  "job i = triangle soup of seed i with N log-uniform over [1e3, 2e6], 4 area-light quads of "
+                  "emission 10, square image of side log-uniform over [128, 1024] (multiple of 16), spp uniform "
+                  "over {1, 4, 16, 64}")
+
+
+def _job_geometry(job):
+    """(tri_abc) of one batched job; runs in a spawn pool before the GPU is touched."""
+    from mobileraytracer_b200 import scenes
+    return scenes._soup_geometry(job.n_triangles, job.seed)
+
+
+def generate_jobs(jobs, workers: int):
+    """Host scenes of the batched jobs, generated in parallel (spawn pool: no CUDA state is forked)."""
+    import multiprocessing as mp
+    from mobileraytracer_b200 import scenes
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(max(1, workers)) as pool:
+        geoms = pool.map(_job_geometry, jobs, chunksize=1)
+    out = []
+    for job, g in zip(jobs, geoms):
+        s = scenes.Scene()
+        s.tri_abc = g
+        s.tri_material = np.zeros(job.n_triangles, np.int32)
+        s.materials = [scenes._material(kd=(0.8, 0.8, 0.8))]
+        s.lights = scenes._quad_lights(10.0)
+        s.camera = scenes.cli_camera(job.side, job.side)
+        out.append(s)
+    log(f"{len(jobs)} job scenes ({sum(j.n_triangles for j in jobs)} triangles) generated in {time.time() - t0:.1f}s")
+    return out
+
+
+def job_opts(job, capi, spp_offset: int = 0, spp: int | None = None):
+    return capi.render_opts(shader=capi.MRT_SHADER_PATHTRACER, width=job.side, height=job.side,
+                            spp=job.spp if spp is None else spp, spl=1, depth_min=3, depth_max=6, seed=job.seed,
+                            spp_offset=spp_offset)
+
+
+def bench_batched(args):
+    """Config 4: the batched renderer against the plain one-job-per-launch renderer on the same job
+    list.  One step = every job rendered once; value = rays traced / wall time of the step."""
+    from mobileraytracer_b200 import scenes
+    jobs = scenes.batched_jobs(args.jobs)
+    host = generate_jobs(jobs, min(16, os.cpu_count() or 1))
+    import torch
+    import mobileraytracer_b200 as m
+    from mobileraytracer_b200 import capi
+    torch.cuda.set_device(0)
+    ctx = m.Context(0)
+    t0 = time.time()
+    built = [m.Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST) for sc in host]
+    build_s = time.time() - t0
+    arena_bytes = sum(b.device_bytes() for b in built)
+    opts = [job_opts(j, capi) for j in jobs]
+    bm_plain = [torch.zeros(j.side * j.side, dtype=torch.int32, device="cuda") for j in jobs]
+    bm_batch = [torch.zeros(j.side * j.side, dtype=torch.int32, device="cuda") for j in jobs]
+    paths = sum(j.side * j.side * j.spp for j in jobs)
+
+    def plain_step():
+        rays = 0
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for k, j in enumerate(jobs):
+            _, _, st = built[k].render(host[k].camera, opts[k], bitmap=bm_plain[k])
+            rays += st.rays_closest + st.rays_shadow
+        torch.cuda.synchronize()
+        return rays, time.perf_counter() - t
+
+    policy = {"smallest": capi.MRT_BATCH_SMALLEST_FIRST, "fifo": capi.MRT_BATCH_FIFO,
+              "share": capi.MRT_BATCH_EQUAL_SHARE}[args.policy]
+    batch = m.Batch(ctx, max_depth=6, max_spl=1, max_jobs=max(4096, len(jobs)), wave_roots=args.wave_roots,
+                    policy=policy)
+
+    def batch_step():
+        s0 = batch.stats()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for k, j in enumerate(jobs):
+            batch.submit(built[k], host[k].camera, opts[k], bm_batch[k])
+        batch.run()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        batch.completed()
+        s1 = batch.stats()
+        return (s1.rays_closest + s1.rays_shadow) - (s0.rays_closest + s0.rays_shadow), dt, s1.busy_ms - s0.busy_ms
+
+    clocks = ClockSampler(0).__enter__()
+    for _ in range(args.warmup):
+        batch_step()
+    plain_step()
+    clocks.mark()
+    b_rays = b_time = b_busy = 0.0
+    for _ in range(args.steps):
+        r, dt, busy = batch_step()
+        b_rays += r
+        b_time += dt
+        b_busy += busy
+    p_rays = p_time = 0.0
+    for _ in range(args.steps):
+        r, dt = plain_step()
+        p_rays += r
+        p_time += dt
+    clocks.__exit__(None, None, None)
+    same = sum(int(torch.equal(a, b)) for a, b in zip(bm_plain, bm_batch))
+    st = batch.stats()
+    value = b_rays / b_time / 1e6
+    plain_value = p_rays / p_time / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": b_time * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "jobs": len(jobs), "paths_per_step": paths,
+                   "triangles": sum(j.n_triangles for j in jobs), "scene_device_bytes": arena_bytes,
+                   "scene_build_seconds": build_s, "rays_per_step": b_rays / args.steps,
+                   "l2": "inputs (scenes ~GBs) far larger than L2",
+                   "policy": args.policy, "wave_roots": st.wave_roots, "block_threads": st.block_threads,
+                   "blocks_per_sm": st.blocks_per_sm, "autotuner_probes": st.autotuned,
+                   "waves_per_step": st.waves / (args.warmup + args.steps),
+                   "device_busy_fraction": b_busy / 1e3 / b_time},
+        "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_step": p_time * 1e3 / args.steps,
+                  "rays_per_step": p_rays / args.steps, "renderer": "mrt_render per job, device buffers"},
+        "batched_over_plain": value / plain_value,
+        "bitmaps_equal_plain": f"{same}/{len(jobs)}",
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for b in built:
+        b.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 200 frames, or 1 batch)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="frame", choices=["frame", "batched"],
+                    help="frame: the 1920x1080 NoShadows frame (default); batched: the 256-job batch")
+    ap.add_argument("--jobs", type=int, default=256, help="batched: jobs in the list")
+    ap.add_argument("--wave-roots", type=int, default=0, help="batched: camera paths per wave (0: autotuned)")
+    ap.add_argument("--policy", default="smallest", choices=["smallest", "fifo", "share"],
+                    help="batched: which jobs fill a wave")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 1 if args.workload == "batched" else 200
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batched":
+        bench_batched(args)
         return
 
     import torch

@@ -20,6 +20,8 @@
  *                         shade() (app/Components/Shaders/{NoShadows,Whitted,PathTracer}.cpp)
  *   mrt_render_stop       Renderer::stopRender()                     (app/MobileRT/Renderer.cpp:61-65)
  *   mrt_render_progress   Renderer::getSample()                      (app/MobileRT/Renderer.cpp:118-120)
+ * mrt_render_noalloc and the mrt_batch_* calls have no counterpart in the reference (the reference
+ * renders one frame per Renderer::renderFrame call).
  */
 #ifndef MRT_CUDA_H
 #define MRT_CUDA_H
@@ -243,6 +245,77 @@ int mrt_render_noalloc(MrtScene *scene, const MrtCamera *camera, const MrtRender
                        uint32_t stride_bytes, float *accum, MrtRenderStats *stats);
 void mrt_render_stop(MrtScene *scene);
 uint32_t mrt_render_progress(const MrtScene *scene);
+
+/* ---- batched rendering (no counterpart in the reference) ------------------------------------ */
+/* Many renders of different scenes, cameras, resolutions and spp as one stream of waves over a
+ * common ray pool.  Each wave takes camera paths from the jobs that still have some (by the
+ * batch's policy), traces them through all bounce levels and folds their values into each job's
+ * bitmap; the wave's kernel sequence is captured once as a CUDA graph and replayed, and several
+ * waves run at once on their own streams (the tail of one wave's bounce levels overlaps the bulk of
+ * another's).  A job's bitmap and sums end bit for bit as mrt_render(..., MRT_MEM_DEVICE, ...) with
+ * the same arguments would leave them (the per-pixel sample order is kept).  Jobs render scenes built with MRT_ACCEL_BVH + MRT_BVH_FAST on the batch's device, with the
+ * plain-rectangle block schedule (width a multiple of 16, stride_bytes = 4 * width and
+ * height / (height / 16) == 16); bitmap and accum are device pointers that stay valid, and scenes
+ * stay alive, until the job is reported done. */
+typedef struct MrtBatch MrtBatch;
+
+typedef struct MrtBatchOpts {
+    uint32_t wave_roots;     /* camera paths per wave; 0 = chosen by the autotuner */
+    uint32_t block_threads;  /* threads per block of the traversal kernels: 64, 128 or 256; 0 = autotuner */
+    uint32_t blocks_per_sm;  /* blocks per SM of the traversal kernels (1..16); 0 = autotuner */
+    uint32_t max_jobs;       /* jobs outstanding at once (job table slots); 0 = 4096 */
+    uint32_t max_depth;      /* largest depth_max of any job (sizes the ray pool); 0 = 8 */
+    uint32_t max_spl;        /* largest samplesLight of any job (sizes the shadow queue); 0 = 4 */
+    uint32_t no_graph;       /* 1: launch each wave's kernels one by one instead of a CUDA graph */
+    uint32_t max_wave_roots; /* upper bound for the autotuner's wave size; 0 = 2^21 */
+    uint32_t policy;         /* MRT_BATCH_SMALLEST_FIRST (0), MRT_BATCH_FIFO or MRT_BATCH_EQUAL_SHARE */
+    uint32_t pipelines;      /* waves in flight at once (1..4), each with its own stream and ray pool;
+                                0 = autotuner (buffers for 4 are allocated) */
+} MrtBatchOpts;
+
+/* Which jobs fill a wave: the fewest paths left first / submission order / an equal share each. */
+#define MRT_BATCH_SMALLEST_FIRST 0
+#define MRT_BATCH_FIFO 1
+#define MRT_BATCH_EQUAL_SHARE 2
+
+typedef struct MrtBatchJob {
+    MrtScene *scene;
+    MrtCamera camera;
+    MrtRenderOpts opts;
+    uint32_t *bitmap;        /* device pointer, 4-byte aligned: running mean as in mrt_render */
+    uint32_t stride_bytes;
+    float *accum;            /* device pointer (16-byte aligned) or NULL: per-pixel fp32 sums */
+} MrtBatchJob;
+
+typedef struct MrtBatchStats {
+    uint64_t rays_closest;   /* closest-hit rays traced by completed and running waves */
+    uint64_t rays_shadow;
+    uint64_t paths;          /* camera paths of the waves launched */
+    uint64_t waves;          /* waves launched */
+    uint64_t jobs_submitted;
+    uint64_t jobs_done;
+    double busy_ms;          /* device time with waves in flight (completed waves) */
+    uint32_t wave_roots;     /* the settings in use (after autotuning) */
+    uint32_t block_threads;
+    uint32_t blocks_per_sm;
+    uint32_t autotuned;      /* candidates the autotuner timed (0: fixed settings) */
+    uint32_t pipelines;
+    uint32_t reserved;
+} MrtBatchStats;
+
+int mrt_batch_create(MrtContext *ctx, const MrtBatchOpts *opts, MrtBatch **out);
+/* Waits for the batch's work on the device, then frees it. */
+void mrt_batch_destroy(MrtBatch *batch);
+/* Queue a job; its paths join the next wave.  MRT_ERR_LIMIT when max_jobs are outstanding. */
+int mrt_batch_submit(MrtBatch *batch, const MrtBatchJob *job, uint64_t *job_id);
+/* Launch up to max_waves waves without waiting for them (at most 8 run ahead of the host);
+ * *launched receives the count (0: no job has paths left). */
+int mrt_batch_step(MrtBatch *batch, uint32_t max_waves, uint32_t *launched);
+/* Ids of jobs that completed since the last call (their bitmap and sums are final). */
+int mrt_batch_completed(MrtBatch *batch, uint64_t *ids, uint32_t capacity, uint32_t *count);
+/* Step until every submitted job is done, then synchronize. */
+int mrt_batch_run(MrtBatch *batch);
+int mrt_batch_stats(const MrtBatch *batch, MrtBatchStats *stats);
 
 #ifdef __cplusplus
 }

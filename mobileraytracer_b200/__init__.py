@@ -19,7 +19,7 @@ import numpy as np
 
 from . import capi
 
-__all__ = ["Context", "Scene", "MrtError", "capi"]
+__all__ = ["Context", "Scene", "Batch", "MrtError", "capi"]
 
 RAY_DTYPE = np.dtype([("origin", np.float32, 3), ("direction", np.float32, 3), ("depth", np.int32),
                       ("exclude", np.uint32)])
@@ -56,6 +56,7 @@ class Context:
         self.h = h
         self.device = device
         self._scenes = weakref.WeakSet()
+        self._batches = weakref.WeakSet()
 
     def check(self, st: int, what: str):
         if st != capi.MRT_OK:
@@ -69,8 +70,10 @@ class Context:
         return int(self.lib.mrt_context_stream(self.h) or 0)
 
     def close(self):
-        """Destroys the context; scenes still open on it are destroyed first."""
+        """Destroys the context; batches and scenes still open on it are destroyed first."""
         if getattr(self, "h", None):
+            for b in list(getattr(self, "_batches", ())):
+                b.close()
             for s in list(getattr(self, "_scenes", ())):
                 s.close()
             self.lib.mrt_context_destroy(self.h)
@@ -183,6 +186,89 @@ class Scene:
             if self.ctx.h:   # a closed context already destroyed its scenes
                 self.lib.mrt_scene_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many renders as one stream of waves over a common ray pool (MrtBatch).
+
+    Jobs are (scene, camera, options, device bitmap, device sums); each ends bit for bit as
+    Scene.render with the same arguments on device buffers would leave it.  Scenes and buffers of a
+    job must stay alive until the job is reported done."""
+
+    def __init__(self, ctx: Context, wave_roots: int = 0, block_threads: int = 0, blocks_per_sm: int = 0,
+                 max_jobs: int = 0, max_depth: int = 0, max_spl: int = 0, graph: bool = True,
+                 max_wave_roots: int = 0, policy: int = capi.MRT_BATCH_SMALLEST_FIRST, pipelines: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        o = capi.MrtBatchOpts()
+        o.wave_roots, o.block_threads, o.blocks_per_sm = wave_roots, block_threads, blocks_per_sm
+        o.max_jobs, o.max_depth, o.max_spl = max_jobs, max_depth, max_spl
+        o.no_graph = 0 if graph else 1
+        o.max_wave_roots = max_wave_roots
+        o.policy = policy
+        o.pipelines = pipelines
+        h = ctypes.c_void_p()
+        ctx.check(self.lib.mrt_batch_create(ctx.h, ctypes.byref(o), ctypes.byref(h)), "mrt_batch_create")
+        self.h = h
+        self._keep = {}
+        ctx._batches.add(self)
+
+    def submit(self, scene: Scene, camera, opts, bitmap, accum=None, stride_bytes: int | None = None) -> int:
+        """Queue one render; bitmap (and accum) are CUDA tensors.  Returns the job id."""
+        if not _is_torch_cuda(bitmap) or (accum is not None and not _is_torch_cuda(accum)):
+            raise MrtError(capi.MRT_ERR_ARG, "Batch.submit takes device (CUDA tensor) buffers")
+        j = capi.MrtBatchJob()
+        j.scene = scene.h.value
+        j.camera = camera
+        j.opts = opts
+        j.bitmap = bitmap.data_ptr()
+        j.stride_bytes = opts.width * 4 if stride_bytes is None else stride_bytes
+        j.accum = accum.data_ptr() if accum is not None else None
+        jid = ctypes.c_uint64()
+        self.ctx.check(self.lib.mrt_batch_submit(self.h, ctypes.byref(j), ctypes.byref(jid)), "mrt_batch_submit")
+        self._keep[jid.value] = (scene, bitmap, accum)
+        return jid.value
+
+    def step(self, max_waves: int = 1) -> int:
+        n = ctypes.c_uint32()
+        self.ctx.check(self.lib.mrt_batch_step(self.h, max_waves, ctypes.byref(n)), "mrt_batch_step")
+        return n.value
+
+    def completed(self) -> list[int]:
+        """Ids of the jobs finished since the last call."""
+        out = []
+        buf = (ctypes.c_uint64 * 256)()
+        while True:
+            n = ctypes.c_uint32()
+            self.ctx.check(self.lib.mrt_batch_completed(self.h, buf, 256, ctypes.byref(n)), "mrt_batch_completed")
+            out += list(buf[:n.value])
+            if n.value < 256:
+                break
+        for jid in out:
+            self._keep.pop(jid, None)
+        return out
+
+    def run(self):
+        """Render every submitted job to completion."""
+        self.ctx.check(self.lib.mrt_batch_run(self.h), "mrt_batch_run")
+
+    def stats(self) -> capi.MrtBatchStats:
+        s = capi.MrtBatchStats()
+        self.ctx.check(self.lib.mrt_batch_stats(self.h, ctypes.byref(s)), "mrt_batch_stats")
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            if self.ctx.h:
+                self.lib.mrt_batch_destroy(self.h)
+            self.h = None
+            self._keep = {}
 
     def __del__(self):
         try:

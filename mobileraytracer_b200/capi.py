@@ -23,6 +23,7 @@ MRT_CAMERA_PERSPECTIVE = 0
 MRT_PRIM_PLANE, MRT_PRIM_SPHERE, MRT_PRIM_TRIANGLE, MRT_PRIM_LIGHT = 0, 1, 2, 3
 MRT_HIT_NONE = 0xFFFFFFFF
 MRT_MEM_HOST, MRT_MEM_DEVICE = 0, 1
+MRT_BATCH_SMALLEST_FIRST, MRT_BATCH_FIFO, MRT_BATCH_EQUAL_SHARE = 0, 1, 2
 RAY_LENGTH_MAX = 1.0e30
 
 STATUS_NAMES = {0: "MRT_OK", 1: "MRT_ERR_ARG", 2: "MRT_ERR_OOM", 3: "MRT_ERR_CUDA", 4: "MRT_ERR_LIMIT",
@@ -97,6 +98,26 @@ class MrtRenderStats(ctypes.Structure):
                 ("device_ms", ctypes.c_float)]
 
 
+class MrtBatchOpts(ctypes.Structure):
+    _fields_ = [("wave_roots", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                ("max_spl", ctypes.c_uint32), ("no_graph", ctypes.c_uint32), ("max_wave_roots", ctypes.c_uint32),
+                ("policy", ctypes.c_uint32), ("pipelines", ctypes.c_uint32)]
+
+
+class MrtBatchJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("camera", MrtCamera), ("opts", MrtRenderOpts),
+                ("bitmap", ctypes.c_void_p), ("stride_bytes", ctypes.c_uint32), ("accum", ctypes.c_void_p)]
+
+
+class MrtBatchStats(ctypes.Structure):
+    _fields_ = [("rays_closest", ctypes.c_uint64), ("rays_shadow", ctypes.c_uint64), ("paths", ctypes.c_uint64),
+                ("waves", ctypes.c_uint64), ("jobs_submitted", ctypes.c_uint64), ("jobs_done", ctypes.c_uint64),
+                ("busy_ms", ctypes.c_double), ("wave_roots", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("autotuned", ctypes.c_uint32), ("pipelines", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
 def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1, pixel_sampler=None,
                 constant_value=0.5, light_sampler=MRT_SAMPLER_RANDOM, rr_sampler=MRT_SAMPLER_RANDOM,
                 depth_min=4, depth_max=8, seed=0, spp_offset=0) -> MrtRenderOpts:
@@ -144,6 +165,13 @@ def load() -> ctypes.CDLL:
                                       P(MrtRenderStats)]),
         "mrt_render_noalloc": (ctypes.c_int, [vp, P(MrtCamera), P(MrtRenderOpts), vp, ctypes.c_uint32, vp,
                                               P(MrtRenderStats)]),
+        "mrt_batch_create": (ctypes.c_int, [vp, P(MrtBatchOpts), P(vp)]),
+        "mrt_batch_destroy": (None, [vp]),
+        "mrt_batch_submit": (ctypes.c_int, [vp, P(MrtBatchJob), P(ctypes.c_uint64)]),
+        "mrt_batch_step": (ctypes.c_int, [vp, ctypes.c_uint32, P(ctypes.c_uint32)]),
+        "mrt_batch_completed": (ctypes.c_int, [vp, P(ctypes.c_uint64), ctypes.c_uint32, P(ctypes.c_uint32)]),
+        "mrt_batch_run": (ctypes.c_int, [vp]),
+        "mrt_batch_stats": (ctypes.c_int, [vp, P(MrtBatchStats)]),
         "mrt_render_stop": (None, [vp]),
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
     }
@@ -159,5 +187,6 @@ EXPORTED_SYMBOLS = [
     "mrt_context_create", "mrt_context_destroy", "mrt_context_error", "mrt_context_synchronize",
     "mrt_context_stream", "mrt_scene_create", "mrt_scene_destroy", "mrt_scene_build", "mrt_scene_device_bytes",
     "mrt_scene_accel_info", "mrt_trace_closest", "mrt_trace_any", "mrt_trace_closest_counts", "mrt_render",
-    "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress",
+    "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress", "mrt_batch_create", "mrt_batch_destroy",
+    "mrt_batch_submit", "mrt_batch_step", "mrt_batch_completed", "mrt_batch_run", "mrt_batch_stats",
 ]

@@ -27,6 +27,9 @@ struct MrtContext {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];
+    // render scratch shared by the context's scenes (renders on one context are serialised on its
+    // stream): wavefront queues, per-sample values, host-path bitmap staging
+    DevBuf wave[8];
 };
 
 struct RefBvhHost {
@@ -55,7 +58,7 @@ struct MrtScene {
     // render state
     std::atomic<uint32_t> progress{0};
     std::atomic<int> stop{0};
-    DevBuf work[8];                     // render scratch (wavefront pools, per-pixel buffers)
+    DevBuf work[1];                     // the scene's explicit pixel-task list (irregular image sizes)
     void *plan_cache = nullptr;         // pixel schedule of the last (width, height, pitch)
     void (*plan_cache_free)(void *) = nullptr;
     ~MrtScene() {

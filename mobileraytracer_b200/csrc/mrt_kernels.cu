@@ -72,6 +72,10 @@ struct TraceWork {
     uint32_t *ctr;
     __device__ uint32_t total() const { return n; }
     __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ bool begin(uint32_t item, TraceLane &lane, Ray &r) const {
         lane.i = item;
         r = load_ray(rays, item);
@@ -97,6 +101,10 @@ struct AnyWork {
     uint32_t *ctr;
     __device__ uint32_t total() const { return n; }
     __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ bool begin(uint32_t item, TraceLane &lane, Ray &r, float &d) const {
         lane.i = item;
         r = load_ray(rays, item);

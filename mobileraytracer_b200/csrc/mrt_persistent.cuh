@@ -73,8 +73,8 @@ __device__ __forceinline__ bool trav_finished(const FastTrav &t) {
 }
 
 // one node step: pop (with distance culling) or expand the current pair
-template <bool kCount>
-__device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t, TravStack &st) {
+template <bool kCount, class S>
+__device__ __forceinline__ void trav_node_step(const S &s, FastTrav &t, TravStack &st) {
     if (t.pair == kPairNone) {
         while (t.sp > 0) {
             --t.sp;
@@ -122,8 +122,8 @@ __device__ __forceinline__ void trav_node_step(const DevScene &s, FastTrav &t, T
     }
 }
 
-template <bool kCount>
-__device__ __forceinline__ void trav_leaf_step(const DevScene &s, const Ray &r, FastTrav &t) {
+template <bool kCount, class S>
+__device__ __forceinline__ void trav_leaf_step(const S &s, const Ray &r, FastTrav &t) {
     FastCounts cnt{0, 0};
     fast_leaf<kCount>(s, r, t.leaf0_first, t.leaf0_count, t.best_t, t.best_i, t.have, cnt);
     if (t.n_leaf > 1) fast_leaf<kCount>(s, r, t.leaf1_first, t.leaf1_count, t.best_t, t.best_i, t.have, cnt);
@@ -134,6 +134,10 @@ __device__ __forceinline__ void trav_leaf_step(const DevScene &s, const Ray &r, 
 // ---------------------------------------------------------------------------------------------
 // the persistent loop.  Work provides:
 //   uint32_t total() const; uint32_t *counter() const;
+//   const DevScene &scene(const Lane &lane, const DevScene &s) -> the scene the lane's ray is
+//        traced in (s itself for a single-scene launch; the lane's job scene in a batch)
+//   view(lane, s) -> what the node and leaf steps read of that scene (s itself, or a FastView
+//        the lane keeps in registers)
 //   bool begin(uint32_t item, Lane &lane, Ray &r)     -> false: nothing to trace for this item
 //   bool finish(Lane &lane, Ray &r, bool hit, float t, uint32_t id, const FastTrav &tr)
 //        -> true: r holds the item's next ray (same lane continues)
@@ -173,7 +177,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             if (!active) {
                 const uint32_t item = base + __popc(idle & ((1u << lane_id) - 1u));
                 if (item < total && work.begin(item, lane, r)) {
-                    start_ray<kCount, Work, Lane>(s, r, t, len0, id0);
+                    start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t, len0, id0);
                     active = true;
                 }
             }
@@ -186,18 +190,18 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
         for (;;) {
             const bool w = active && trav_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) trav_node_step<kCount>(s, t, stk);
+            if (w) trav_node_step<kCount>(work.view(lane, s), t, stk);
         }
         // 3. leaf phase
-        if (active && t.n_leaf > 0) trav_leaf_step<kCount>(s, r, t);
+        if (active && t.n_leaf > 0) trav_leaf_step<kCount>(work.view(lane, s), r, t);
         // 4. completion
         if (active && trav_finished(t)) {
             float len = len0;
             uint32_t id = id0;
             if (t.have) { len = t.best_t; id = hid(MRT_PRIM_TRIANGLE, t.best_i); }
-            const bool hit_light = lights_trace(s, r, len, id);
+            const bool hit_light = lights_trace(work.scene(lane, s), r, len, id);
             const bool hit = id != MRT_HIT_NONE || hit_light;
-            if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(s, r, t, len0, id0);
+            if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t, len0, id0);
             else active = false;
         }
     }
@@ -210,7 +214,7 @@ namespace mrt {
 // ---------------------------------------------------------------------------------------------
 // any-hit (Shader::shadowTrace, Shader.cpp:162-187): planes and spheres in order, then the tree;
 // the first occluder ends the ray, so no ordering and no distance culling beyond `dist`.
-// Work provides total(), counter(), begin(item, lane, r, dist) and finish(lane, occluded).
+// Work provides total(), counter(), scene(lane, s), begin(item, lane, r, dist) and finish(lane, occluded).
 // ---------------------------------------------------------------------------------------------
 struct OccTrav {
     FastRay f;
@@ -250,7 +254,8 @@ __device__ __forceinline__ bool occ_finished(const OccTrav &t) {
     return t.occluded || (t.n_leaf == 0 && t.pair == kPairNone && t.sp == 0);
 }
 
-__device__ __forceinline__ void occ_node_step(const DevScene &s, OccTrav &t, uint32_t *stack_n) {
+template <class S>
+__device__ __forceinline__ void occ_node_step(const S &s, OccTrav &t, uint32_t *stack_n) {
     if (t.pair == kPairNone) {
         if (t.sp > 0) t.pair = stack_n[--t.sp];
         return;
@@ -288,7 +293,8 @@ __device__ __forceinline__ void occ_node_step(const DevScene &s, OccTrav &t, uin
     }
 }
 
-__device__ __forceinline__ void occ_leaf_step(const DevScene &s, const Ray &r, OccTrav &t) {
+template <class S>
+__device__ __forceinline__ void occ_leaf_step(const S &s, const Ray &r, OccTrav &t) {
     for (int q = 0; q < t.n_leaf && !t.occluded; ++q) {
         const uint32_t first = q == 0 ? t.leaf0_first : t.leaf1_first, count = q == 0 ? t.leaf0_count : t.leaf1_count;
         if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
@@ -325,7 +331,7 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
                 const uint32_t item = base + __popc(idle & ((1u << lane_id) - 1u));
                 float dist;
                 if (item < total && work.begin(item, lane, r, dist)) {
-                    occ_begin(s, r, dist, t);
+                    occ_begin(work.scene(lane, s), r, dist, t);
                     active = true;
                 }
             }
@@ -337,9 +343,9 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
         for (;;) {
             const bool w = active && occ_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) occ_node_step(s, t, stack_n);
+            if (w) occ_node_step(work.view(lane, s), t, stack_n);
         }
-        if (active && t.n_leaf > 0) occ_leaf_step(s, r, t);
+        if (active && t.n_leaf > 0) occ_leaf_step(work.view(lane, s), r, t);
         if (active && occ_finished(t)) {
             work.finish(lane, t.occluded);
             active = false;

@@ -23,104 +23,12 @@
 #include <mutex>
 
 #include "mrt_internal.h"
-#include "mrt_persistent.cuh"
+#include "mrt_wave.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
 
 namespace {
-
-struct Task {
-    uint32_t x, y, index;
-};
-
-struct RenderParams {
-    DevCamera cam;
-    uint32_t width, height, spp, spl, stride_px;
-    int32_t pixel_sampler, light_sampler, rr_sampler, shader;
-    float constant_value;
-    int32_t depth_min, depth_max;
-    uint64_t seed;
-    uint32_t spp_offset;
-    uint32_t strata;       // spp of the whole render (Stratified sampler strata)
-    uint32_t task_base;    // first task of the current round (wavefront)
-    // tasks: implicit rectangle (tasks == nullptr: x = t % width, y = t / width) or explicit list
-    const Task *tasks;
-    uint32_t n_tasks;
-    uint32_t *bitmap;
-    float4 *accum;
-    float inv_w, inv_h, pw, ph;
-};
-
-__device__ __forceinline__ Task task_of(const RenderParams &p, uint32_t t) {
-    if (p.tasks) return p.tasks[t];
-    Task k;
-    k.x = t % p.width;
-    k.y = t / p.width;
-    k.index = k.y * p.stride_px + k.x;
-    return k;
-}
-
-// fp32 sum slot of the bitmap pixel a task writes (a task past the right edge wraps into the next
-// row, as pixelIndex = y * stride + x does in Renderer.cpp:105); -1 when it lands in the row padding
-__device__ __forceinline__ int64_t accum_slot(const RenderParams &p, const Task &k) {
-    const uint32_t row = k.index / p.stride_px, col = k.index - row * p.stride_px;
-    return col < p.width ? (int64_t)row * p.width + col : -1;
-}
-
-__device__ __forceinline__ Ray primary_ray(const RenderParams &p, const Task &k, const Stream &st) {
-    const float u = (float)k.x * p.inv_w, v = (float)k.y * p.inv_h;   // Renderer.cpp:95-99
-    const float r1 = draw(st, p.pixel_sampler, 0u, 0u);
-    const float r2 = draw(st, p.pixel_sampler, 0u, 1u);
-    return camera_ray(p.cam, u, v, (r1 - 0.5f) * 2.0f * p.pw, (r2 - 0.5f) * 2.0f * p.ph);
-}
-
-// Shader::getLight (Shader.cpp:225-236) and Light::getPosition (PointLight.cpp:17-19,
-// AreaLight.cpp:22-31) for light sample j of a node
-__device__ __forceinline__ const DevLight &pick_light(const DevScene &s, const Stream &st, uint32_t node, uint32_t j) {
-    const float u = key_float(st.base, node, kDimLight + 3u * j);
-    const uint32_t k = (uint32_t)floorf(u * (float)s.n_light * 0.99999f);
-    return s.lights[k];
-}
-__device__ __forceinline__ V3 light_position(const DevLight &l, const Stream &st, int kind, uint32_t node, uint32_t j) {
-    if (l.kind != MRT_LIGHT_AREA) return l.pos;
-    float R = draw(st, kind, node, kDimLight + 3u * j + 1u);
-    float S = draw(st, kind, node, kDimLight + 3u * j + 2u);
-    if (R + S >= 1.0f) { R = 1.0f - R; S = 1.0f - S; }
-    return (l.a + l.ab * R) + l.ac * S;
-}
-
-__device__ __forceinline__ bool material_of(const DevScene &s, const Isect &it, DevMaterial &m) {
-    if (it.light >= 0) { m = s.lights[it.light].radiance; return true; }
-    if (it.mat >= 0) { m = s.mats[it.mat]; return true; }
-    return false;
-}
-
-// NoShadows::shade, NoShadows.cpp:19-65
-__device__ __forceinline__ V3 shade_noshadows(const DevScene &s, const RenderParams &p, const Stream &st, const Isect &it,
-                                              uint32_t node) {
-    V3 rgb{0.0f, 0.0f, 0.0f};
-    V3 kd;
-    DevMaterial m;
-    if (material_of(s, it, m)) {
-        if (any_pos(m.le)) return m.le;
-        kd = m.kd;
-    } else {
-        kd = it.color;
-    }
-    if (any_pos(kd) && s.n_light > 0) {
-        for (uint32_t j = 0; j < p.spl; ++j) {
-            const DevLight &l = pick_light(s, st, node, j);
-            const V3 lp = light_position(l, st, p.light_sampler, node, j);
-            const V3 vtl = normalize(lp - it.point);
-            const float c = dot(it.normal, vtl);
-            if (c > 0.0f) rgb = rgb + l.radiance.le * c;
-        }
-        rgb = rgb * kd;
-        rgb = rgb / (float)p.spl;
-    }
-    return rgb + kd * 0.1f;
-}
 
 template <int ACCEL, int MODE>
 __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderParams p, uint32_t round_first,
@@ -171,6 +79,10 @@ struct NsWork {
     uint32_t tiles_x;   // 0: row-major tasks
     __device__ uint32_t total() const { return count; }
     __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ Ray ray_for(const NsLane &lane) const {
         const Stream st = make_stream(p->seed, lane.pixel, p->spp_offset + lane.si, p->strata, p->constant_value);
         return primary_ray(*p, lane.k, st);
@@ -221,83 +133,6 @@ __global__ void __launch_bounds__(128) k_render_noshadows_fast(DevScene s, Rende
 }
 
 // ============================== wavefront ====================================================
-enum NodeKind : uint32_t { kMiss = 0, kEmit = 1, kCut = 2, kShaded = 3 };
-enum NodeFlag : uint32_t { kHasIndirect = 4, kRRScaled = 8, kKdPos = 16, kKsPos = 32, kKtPos = 64 };
-
-struct RayRec {          // 48 bytes
-    float ox, oy, oz, dx, dy, dz;
-    int32_t depth;
-    uint32_t exclude;
-    uint32_t root;       // wave-local root index
-    uint32_t parent;     // node index of the parent (0xFFFFFFFF for camera rays)
-    uint32_t slot;       // 0 indirect, 1 specular, 2 transmission
-    uint32_t code;       // path-tree code keying the stream (root 1, child code*4 + slot + 1)
-};
-
-struct NodeRec {         // 128 bytes
-    uint32_t flags;      // kind | NodeFlag
-    uint32_t occluded;   // bit j: shadow ray of light sample j was blocked
-    float hit_t;
-    uint32_t hit_id;
-    V3 kd, ks, kt;       // 36
-    V3 point, normal;    // 24 (or rgb of an emitter in `point`)
-    V3 child[3];         // 36
-    uint32_t child_flag; // bit s: child s reported a light hit
-    uint32_t pad[3];
-};
-
-struct ShadowRec {       // 40 bytes
-    float ox, oy, oz, dx, dy, dz, dist;
-    uint32_t node;
-    uint32_t j;
-    uint32_t exclude;
-};
-
-struct Level {
-    uint32_t start;
-    uint32_t count;
-    uint32_t shadow_count;
-    uint32_t pad;
-};
-
-struct WaveState {
-    RayRec *rays;
-    NodeRec *nodes;
-    ShadowRec *shadows;
-    Level *levels;           // [max_levels + 1]
-    float4 *root_rgb;        // per wave root: rgb, flag
-    uint32_t ray_cap;
-    uint32_t shadow_cap;
-    uint32_t root_first;     // global index of the wave's first root
-    uint32_t n_roots;
-    unsigned long long *counters;   // [0] closest rays, [1] shadow rays
-};
-
-__device__ __forceinline__ uint32_t warp_alloc(uint32_t want, uint32_t *counter) {
-    // warp-aggregated allocation: inclusive scan of `want` across the warp, one atomic per warp.
-    // Every lane of the warp calls this (the shade loop runs whole warps).
-    __syncwarp();
-    const int lane = threadIdx.x & 31;
-    uint32_t incl = want;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    uint32_t base = 0;
-    if (lane == 31 && incl > 0) base = atomicAdd(counter, incl);
-    base = __shfl_sync(0xFFFFFFFFu, base, 31);
-    return base + incl - want;
-}
-
-__device__ __forceinline__ void root_task(const RenderParams &p, const WaveState &w, uint32_t root, Task &k,
-                                          uint32_t &pixel, uint32_t &sample) {
-    const uint32_t g = w.root_first + root;
-    const uint32_t t = p.task_base + g / p.spp, si = g % p.spp;
-    k = task_of(p, t);
-    pixel = k.y * p.width + k.x;
-    sample = p.spp_offset + si;
-}
-
 __global__ void k_wave_raygen(RenderParams p, WaveState w) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n_roots; i += gridDim.x * blockDim.x) {
         Task k;
@@ -322,23 +157,6 @@ __global__ void k_wave_raygen(RenderParams p, WaveState w) {
         w.levels[0].shadow_count = 0;
     }
 }
-
-__device__ __forceinline__ Ray ray_of(const RayRec &r) {
-    Ray x;
-    x.o = V3{r.ox, r.oy, r.oz};
-    x.d = V3{r.dx, r.dy, r.dz};
-    x.depth = r.depth;
-    x.exclude = r.exclude;
-    return x;
-}
-
-__device__ __forceinline__ Level clamp_level(const WaveState &w, Level L) {
-    // a level never reaches past the ray pool (overflowing children were dropped with MRT_ERR_LIMIT)
-    L.start = min(L.start, w.ray_cap);
-    L.count = min(L.count, w.ray_cap - L.start);
-    return L;
-}
-
 template <int ACCEL, int MODE>
 __global__ void __launch_bounds__(128) k_wave_extend(DevScene s, WaveState w, int level) {
     const Level L = clamp_level(w, w.levels[level]);
@@ -364,140 +182,27 @@ __global__ void __launch_bounds__(128) k_wave_shade(DevScene s, RenderParams p, 
         const uint32_t i = it_ * blockDim.x + threadIdx.x;
         const bool active = i < L.count;
         const uint32_t idx = L.start + (active ? i : 0);
-        uint32_t n_child = 0, n_shadow = 0;
-        Ray child[3];
-        uint32_t child_slot[3];
-        NodeRec nd;
+        ShadeLane o;
+        o.n_child = 0;
+        o.n_shadow = 0;
+        o.shaded = false;
         RayRec rr;
-        Isect isect;
         Stream st;
-        bool shaded = false;
         if (active) {
             rr = w.rays[idx];
-            const Ray r = ray_of(rr);
-            nd.flags = kMiss;
-            nd.occluded = 0;
-            nd.child_flag = 0;
-            nd.child[0] = nd.child[1] = nd.child[2] = V3{0, 0, 0};
-            nd.kd = nd.ks = nd.kt = V3{0, 0, 0};
-            nd.point = nd.normal = V3{0, 0, 0};
-            const uint32_t hit_id = w.nodes[idx].hit_id;
-            nd.hit_id = hit_id;
-            nd.hit_t = w.nodes[idx].hit_t;
             Task k;
             uint32_t pixel, sample;
             root_task(p, w, rr.root, k, pixel, sample);
             st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
-            if (hit_id != MRT_HIT_NONE && make_isect(s, r, hit_id, isect)) {
-                if (r.depth > p.depth_max) {
-                    nd.flags = kCut;   // Whitted.cpp:20-22, PathTracer.cpp:28-31
-                } else {
-                    DevMaterial m;
-                    V3 kd, ks{0, 0, 0}, kt{0, 0, 0};
-                    float ior = 1.0f;
-                    bool emitted = false;
-                    if (material_of(s, isect, m)) {
-                        if (any_pos(m.le)) { nd.flags = kEmit; nd.point = m.le; emitted = true; }
-                        kd = m.kd; ks = m.ks; kt = m.kt; ior = m.ior;
-                    } else {
-                        kd = isect.color;
-                    }
-                    if (!emitted) {
-                        shaded = true;
-                        nd.flags = kShaded;
-                        nd.kd = kd; nd.ks = ks; nd.kt = kt;
-                        nd.point = isect.point;
-                        nd.normal = isect.normal;
-                        const bool kd_pos = any_pos(kd), ks_pos = any_pos(ks), kt_pos = any_pos(kt);
-                        if (kd_pos) nd.flags |= kKdPos;
-                        if (ks_pos) nd.flags |= kKsPos;
-                        if (kt_pos) nd.flags |= kKtPos;
-                        if (kd_pos && s.n_light > 0) {
-                            for (uint32_t j = 0; j < p.spl; ++j) {
-                                const DevLight &l = pick_light(s, st, rr.code, j);
-                                const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
-                                const V3 vtl = normalize(lp - isect.point);
-                                if (dot(isect.normal, vtl) > 0.0f) ++n_shadow;
-                            }
-                        }
-                        if (p.shader == MRT_SHADER_PATHTRACER && kd_pos) {
-                            bool go = r.depth <= p.depth_min;   // PathTracer.cpp:106-107
-                            if (!go) go = draw(st, p.rr_sampler, rr.code, kDimRR) > 0.5f;
-                            if (go) {
-                                nd.flags |= kHasIndirect;
-                                if (r.depth > p.depth_min) nd.flags |= kRRScaled;
-                                Ray c;
-                                c.o = isect.point;
-                                c.d = hemisphere(isect.normal, key_float(st.base, rr.code, kDimHemi),
-                                                 key_float(st.base, rr.code, kDimHemi + 1u));
-                                c.depth = r.depth + 1;
-                                c.exclude = isect.prim;
-                                child[n_child] = c;
-                                child_slot[n_child++] = 0;
-                            }
-                        }
-                        if (ks_pos) {
-                            Ray c;
-                            c.o = isect.point;
-                            c.d = reflect(r.d, isect.normal);
-                            c.depth = r.depth + 1;
-                            c.exclude = isect.prim;
-                            child[n_child] = c;
-                            child_slot[n_child++] = 1;
-                        }
-                        if (kt_pos) {
-                            Ray c;
-                            c.o = isect.point;
-                            c.d = refract(r.d, isect.normal, 1.0f / ior);
-                            c.depth = r.depth + 1;
-                            c.exclude = isect.prim;
-                            child[n_child] = c;
-                            child_slot[n_child++] = 2;
-                        }
-                    }
-                }
-            }
-            w.nodes[idx] = nd;
+            shade_ray(s, p, rr, w.nodes[idx].hit_id, w.nodes[idx].hit_t, st, o);
+            w.nodes[idx] = o.nd;
         }
         // queue compaction: one atomic per warp for children, one for shadow rays
-        const uint32_t cbase = warp_alloc(n_child, &next->count);
-        const uint32_t sbase = warp_alloc(n_shadow, &w.levels[level].shadow_count);
+        const uint32_t cbase = warp_alloc(o.n_child, &next->count);
+        const uint32_t sbase = warp_alloc(o.n_shadow, &w.levels[level].shadow_count);
         if (!active) continue;
-        for (uint32_t c = 0; c < n_child; ++c) {
-            const uint32_t pos = next_start + cbase + c;
-            if (pos >= w.ray_cap) { raise_error(s, MRT_ERR_LIMIT); break; }
-            RayRec o;
-            o.ox = child[c].o.x; o.oy = child[c].o.y; o.oz = child[c].o.z;
-            o.dx = child[c].d.x; o.dy = child[c].d.y; o.dz = child[c].d.z;
-            o.depth = child[c].depth;
-            o.exclude = child[c].exclude;
-            o.root = rr.root;
-            o.parent = idx;
-            o.slot = child_slot[c];
-            o.code = rr.code * 4u + child_slot[c] + 1u;
-            w.rays[pos] = o;
-        }
-        if (shaded && n_shadow) {
-            uint32_t q = 0;
-            for (uint32_t j = 0; j < p.spl; ++j) {
-                const DevLight &l = pick_light(s, st, rr.code, j);
-                const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
-                V3 vtl = lp - isect.point;
-                const float dist = length(vtl);
-                vtl = normalize(vtl);
-                if (!(dot(isect.normal, vtl) > 0.0f)) continue;
-                const uint32_t pos = sbase + q++;
-                if (pos >= w.shadow_cap) { raise_error(s, MRT_ERR_LIMIT); break; }
-                ShadowRec sr;
-                sr.ox = isect.point.x; sr.oy = isect.point.y; sr.oz = isect.point.z;
-                sr.dx = vtl.x; sr.dy = vtl.y; sr.dz = vtl.z;
-                sr.dist = dist;
-                sr.node = idx;
-                sr.j = j;
-                sr.exclude = isect.prim;
-                w.shadows[pos] = sr;
-            }
-        }
+        emit_children(s, o, rr, idx, next_start + cbase, w.rays, w.ray_cap);
+        emit_shadows(s, p, st, o, rr, idx, sbase, w.shadows, w.shadow_cap);
     }
 }
 
@@ -526,6 +231,10 @@ struct ExtendWork {
     uint32_t *ctr;
     __device__ uint32_t total() const { return L.count; }
     __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ bool begin(uint32_t item, WaveLane &lane, Ray &r) const {
         lane.idx = L.start + item;
         r = ray_of(w.rays[lane.idx]);
@@ -543,6 +252,10 @@ struct ShadowWork {
     uint32_t *ctr;
     __device__ uint32_t total() const { return n; }
     __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ bool begin(uint32_t item, WaveLane &lane, Ray &r, float &dist) const {
         const ShadowRec sr = w.shadows[item];
         lane.idx = item;
@@ -584,51 +297,13 @@ __global__ void __launch_bounds__(128) k_wave_resolve(DevScene s, RenderParams p
         const uint32_t idx = L.start + i;
         const NodeRec nd = w.nodes[idx];
         const RayRec rr = w.rays[idx];
-        V3 rgb{0.0f, 0.0f, 0.0f};
-        bool flag = false;
-        const uint32_t kind = nd.flags & 3u;
-        if (kind == kEmit) {
-            rgb = nd.point;
-            flag = true;
-        } else if (kind == kShaded) {
-            Task k;
-            uint32_t pixel, sample;
-            root_task(p, w, rr.root, k, pixel, sample);
-            const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
-            V3 direct{0.0f, 0.0f, 0.0f};
-            const bool kd_pos = (nd.flags & kKdPos) != 0;
-            if (kd_pos && s.n_light > 0) {
-                for (uint32_t j = 0; j < p.spl; ++j) {
-                    const DevLight &l = pick_light(s, st, rr.code, j);
-                    const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
-                    const V3 vtl = normalize(lp - nd.point);
-                    const float c = dot(nd.normal, vtl);
-                    if (c > 0.0f && !((nd.occluded >> (j & 31u)) & 1u)) direct = direct + l.radiance.le * c;
-                }
-                direct = direct * nd.kd;
-                direct = direct / (float)p.spl;
-            }
-            if (p.shader == MRT_SHADER_WHITTED) {   // Whitted.cpp:64-106
-                rgb = direct;
-                if (nd.flags & kKsPos) rgb = rgb + nd.ks * nd.child[1];
-                if (nd.flags & kKtPos) rgb = rgb + nd.kt * nd.child[2];
-                rgb = rgb + nd.kd * 0.1f;
-            } else {   // PathTracer.cpp:100-163
-                V3 lid{0.0f, 0.0f, 0.0f}, lis{0.0f, 0.0f, 0.0f}, lit{0.0f, 0.0f, 0.0f};
-                if (nd.flags & kHasIndirect) {
-                    lid = lid + nd.kd * nd.child[0];
-                    if (nd.flags & kRRScaled) lid = lid / (0.5f * 0.5f);
-                    flag = (nd.child_flag & 1u) != 0;
-                    if (any_pos(direct) && flag) lid = V3{0.0f, 0.0f, 0.0f};
-                }
-                if (nd.flags & kKsPos) lis = lis + nd.ks * nd.child[1];
-                if (nd.flags & kKtPos) lit = lit + nd.kt * nd.child[2];
-                rgb = rgb + direct;
-                rgb = rgb + lid;
-                rgb = rgb + lis;
-                rgb = rgb + lit;
-            }
-        }
+        Task k;
+        uint32_t pixel, sample;
+        root_task(p, w, rr.root, k, pixel, sample);
+        const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+        V3 rgb;
+        bool flag;
+        resolve_node(s, p, nd, rr, st, rgb, flag);
         if (rr.parent == 0xFFFFFFFFu) {
             w.root_rgb[rr.root] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
         } else {
@@ -872,20 +547,20 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         const uint64_t shadow_cap = (uint64_t)wave * std::max(1u, o->spl) * 2ull;
         if (ray_cap > 0xFFFFFFF0ull) { set_error(ctx, "mrt_render: wave too large"); return MRT_ERR_ARG; }
         if (2 * (levels + 1) > 64) { set_error(ctx, "mrt_render: depth_max above 30"); return MRT_ERR_ARG; }
-        if (st == MRT_OK) st = ensure(ctx, s->work[1], sizeof(RayRec) * ray_cap);
-        if (st == MRT_OK) st = ensure(ctx, s->work[2], sizeof(NodeRec) * ray_cap);
-        if (st == MRT_OK) st = ensure(ctx, s->work[3], sizeof(ShadowRec) * shadow_cap);
-        if (st == MRT_OK) st = ensure(ctx, s->work[4], sizeof(Level) * (levels + 2));
-        if (st == MRT_OK) st = ensure(ctx, s->work[5], sizeof(float4) * wave);
-        if (st == MRT_OK) st = ensure(ctx, s->work[6], 16);
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[1], sizeof(RayRec) * ray_cap);
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[2], sizeof(NodeRec) * ray_cap);
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[3], sizeof(ShadowRec) * shadow_cap);
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[4], sizeof(Level) * (levels + 2));
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[5], sizeof(float4) * wave);
+        if (st == MRT_OK) st = ensure(ctx, ctx->wave[6], 16);
         if (st != MRT_OK) return st;
         WaveState w{};
-        w.rays = (RayRec *)s->work[1].ptr;
-        w.nodes = (NodeRec *)s->work[2].ptr;
-        w.shadows = (ShadowRec *)s->work[3].ptr;
-        w.levels = (Level *)s->work[4].ptr;
-        w.root_rgb = (float4 *)s->work[5].ptr;
-        w.counters = (unsigned long long *)s->work[6].ptr;
+        w.rays = (RayRec *)ctx->wave[1].ptr;
+        w.nodes = (NodeRec *)ctx->wave[2].ptr;
+        w.shadows = (ShadowRec *)ctx->wave[3].ptr;
+        w.levels = (Level *)ctx->wave[4].ptr;
+        w.root_rgb = (float4 *)ctx->wave[5].ptr;
+        w.counters = (unsigned long long *)ctx->wave[6].ptr;
         w.ray_cap = (uint32_t)ray_cap;
         w.shadow_cap = (uint32_t)shadow_cap;
         cudaMemsetAsync(w.counters, 0, 16, q);
@@ -963,10 +638,10 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
         return MRT_ERR_ARG;
     }
     if (mem == MRT_MEM_HOST) {
-        st = ensure(ctx, s->work[7], acc_offset + (accum ? acc_bytes : 0));
+        st = ensure(ctx, ctx->wave[7], acc_offset + (accum ? acc_bytes : 0));
         if (st != MRT_OK) return st;
-        d_bitmap = (uint32_t *)s->work[7].ptr;
-        d_accum = accum ? (float *)((char *)s->work[7].ptr + acc_offset) : nullptr;
+        d_bitmap = (uint32_t *)ctx->wave[7].ptr;
+        d_accum = accum ? (float *)((char *)ctx->wave[7].ptr + acc_offset) : nullptr;
         st = cuda_status(ctx, cudaMemcpyAsync(d_bitmap, bitmap, bm_bytes, cudaMemcpyHostToDevice, ctx->stream), "bitmap in");
         if (st == MRT_OK && accum)
             st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");

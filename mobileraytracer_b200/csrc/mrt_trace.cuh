@@ -21,8 +21,23 @@ constexpr uint32_t kMaxBvhSteps = 1u << 24;   // traversal iterations per ray be
 
 MRT_HD uint32_t hid(uint32_t type, uint32_t index) { return MRT_HIT_ID(type, index); }
 
-__device__ __forceinline__ void raise_error(const DevScene &s, int code) {
+template <class S>
+__device__ __forceinline__ void raise_error(const S &s, int code) {
     if (s.error_flag) atomicMax(s.error_flag, code);
+}
+
+// the fields of a scene the FAST-BVH node and leaf steps read; a persistent lane that traces in a
+// scene of its own (batched jobs) keeps these in registers instead of re-reading its scene record
+struct FastView {
+    const float4 *fnodes;
+    const float4 *ftris;
+    uint32_t n_fnodes;
+    uint32_t n_tri;
+    int32_t *error_flag;
+};
+
+__device__ __forceinline__ FastView fast_view(const DevScene &s) {
+    return FastView{s.fnodes, s.ftris, s.n_fnodes, s.n_tri, s.error_flag};
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -350,8 +365,8 @@ struct FastCounts {
     uint32_t tris;   // 48-byte triangle records fetched
 };
 
-template <bool kCount>
-__device__ __forceinline__ void fast_leaf(const DevScene &s, const Ray &r, uint32_t first, uint32_t count,
+template <bool kCount, class S>
+__device__ __forceinline__ void fast_leaf(const S &s, const Ray &r, uint32_t first, uint32_t count,
                                           float &best_t, uint32_t &best_i, bool &have, FastCounts &cnt) {
     if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
     for (uint32_t k = first; k < first + count; ++k) {
