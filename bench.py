@@ -286,7 +286,7 @@ def bench_batched(args):
     policy = {"smallest": capi.MRT_BATCH_SMALLEST_FIRST, "fifo": capi.MRT_BATCH_FIFO,
               "share": capi.MRT_BATCH_EQUAL_SHARE}[args.policy]
     batch = m.Batch(ctx, max_depth=6, max_spl=1, max_jobs=max(4096, len(jobs)), wave_roots=args.wave_roots,
-                    policy=policy)
+                    policy=policy, pipelines=args.pipelines)
 
     def batch_step():
         s0 = batch.stats()
@@ -331,7 +331,7 @@ def bench_batched(args):
                    "scene_build_seconds": build_s, "rays_per_step": b_rays / args.steps,
                    "l2": "inputs (scenes ~GBs) far larger than L2",
                    "policy": args.policy, "wave_roots": st.wave_roots, "block_threads": st.block_threads,
-                   "blocks_per_sm": st.blocks_per_sm, "autotuner_probes": st.autotuned,
+                   "blocks_per_sm": st.blocks_per_sm, "pipelines": st.pipelines, "autotuner_probes": st.autotuned,
                    "waves_per_step": st.waves / (args.warmup + args.steps),
                    "device_busy_fraction": b_busy / 1e3 / b_time},
         "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_step": p_time * 1e3 / args.steps,
@@ -348,6 +348,89 @@ def bench_batched(args):
     ctx.close()
 
 
+SERVE_WORKLOAD = ("config 5: Poisson stream of render requests, each drawn as a batched-workload job (PathTracer "
+                  "depth 6, soup geometry from the 256-job pool, side log-uniform over [128, 1024], spp uniform "
+                  "over {1, 4, 16, 64}); 20% re-render one of the last 64 new scenes with +16 spp progressive "
+                  "accumulation; admission by device footprint")
+
+
+def bench_served(args):
+    """Config 5: the same request stream served by the batched renderer (continuous batching) and by
+    one mrt_render call per request; throughput, p50/p99 latency, offered vs achieved load."""
+    from mobileraytracer_b200 import scenes
+    from mobileraytracer_b200 import serve
+    pool = scenes.batched_jobs(256)
+    host = generate_jobs(pool, min(16, os.cpu_count() or 1))
+    reqs = serve.request_stream(pool, duration_s=args.duration, rate=args.rate)
+    offered_paths = sum(r.paths for r in reqs)
+    log(f"{len(reqs)} requests over {args.duration}s ({sum(r.kind == 'rerender' for r in reqs)} re-renders), "
+        f"{offered_paths / args.duration / 1e6:.1f} M paths/s offered")
+    import torch
+    import mobileraytracer_b200 as m
+    from mobileraytracer_b200 import capi
+    torch.cuda.set_device(0)
+    budget = int(args.budget_gb * 1e9)
+    bitmap_reserve = 8 << 30          # images of every scene served (kept for progressive re-renders)
+    build_slack = 1 << 30             # tree-build scratch of the scene being built
+    scene_budget = budget - bitmap_reserve - build_slack
+
+    def pool_scene(r):
+        return host[r.geometry]
+
+    results = {}
+    clocks = ClockSampler(0).__enter__()
+    clocks.mark()
+    for kind in ("plain", "batched"):
+        ctx = m.Context(0)
+        arena = m.Arena(0, scene_budget + build_slack)
+        if kind == "batched":
+            be = serve.BatchBackend(ctx, arena, pool_scene, dict(
+                max_depth=6, max_spl=1, max_jobs=4096, wave_roots=args.wave_roots or (1 << 20),
+                max_wave_roots=max(args.wave_roots, 1 << 20), block_threads=64, blocks_per_sm=16,
+                pipelines=args.pipelines or 4))
+        else:
+            be = serve.PlainBackend(ctx, arena, pool_scene)
+        loop = serve.ServeLoop(reqs, be, scene_budget)
+        t = time.perf_counter()
+        summary = loop.run()
+        torch.cuda.synchronize()
+        summary["wall_seconds"] = time.perf_counter() - t
+        summary["rays"] = be.total_rays()
+        summary["checksums"] = dict(be.checksums)
+        summary["arena"] = arena.stats()
+        be.close()
+        ctx.close()
+        arena.close()
+        results[kind] = summary
+        log(f"{kind}: {summary['wall_seconds']:.1f}s, p50 {summary['latency_p50_s']:.3f}s p99 "
+            f"{summary['latency_p99_s']:.3f}s, {summary['rays'] / summary['wall_seconds'] / 1e6:.1f} Mrays/s")
+    clocks.__exit__(None, None, None)
+    same = sum(int(results["plain"]["checksums"][i] == results["batched"]["checksums"][i]) for i in range(len(reqs)))
+
+    def summ(r):
+        return {"Mrays_per_s": r["rays"] / r["wall_seconds"] / 1e6, "wall_seconds": r["wall_seconds"],
+                "latency_p50_s": r["latency_p50_s"], "latency_p99_s": r["latency_p99_s"],
+                "latency_mean_s": r["latency_mean_s"], "achieved_paths_per_s": offered_paths / r["wall_seconds"],
+                "rays": r["rays"], "evictions": r["evictions"], "rebuilds_after_eviction": r["rebuilds_after_eviction"],
+                "peak_scene_bytes": r["peak_scene_bytes"], "arena_peak_bytes": r["arena"]["peak"]}
+
+    b, p = summ(results["batched"]), summ(results["plain"])
+    line = {
+        "metric": METRIC, "value": b["Mrays_per_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": b["wall_seconds"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "duration_s": args.duration, "rate_per_s": args.rate,
+                   "requests": len(reqs), "rerenders": sum(r.kind == "rerender" for r in reqs),
+                   "offered_paths_per_s": offered_paths / args.duration, "budget_bytes": budget,
+                   "scene_budget_bytes": scene_budget, "bitmap_reserve_bytes": bitmap_reserve,
+                   "build_slack_bytes": build_slack},
+        "served": b, "plain": p, "served_over_plain": b["Mrays_per_s"] / p["Mrays_per_s"],
+        "results_equal_plain": f"{same}/{len(reqs)}",
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,8 +440,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="frame", choices=["frame", "batched"],
-                    help="frame: the 1920x1080 NoShadows frame (default); batched: the 256-job batch")
+    ap.add_argument("--workload", default="frame", choices=["frame", "batched", "served"],
+                    help="frame: the 1920x1080 NoShadows frame (default); batched: the 256-job batch; "
+                         "served: the request stream")
+    ap.add_argument("--duration", type=float, default=120.0, help="served: seconds of arrivals")
+    ap.add_argument("--rate", type=float, default=50.0, help="served: arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="served: device footprint budget")
+    ap.add_argument("--pipelines", type=int, default=0, help="batched/served: waves in flight (0: autotuned / 4)")
     ap.add_argument("--jobs", type=int, default=256, help="batched: jobs in the list")
     ap.add_argument("--wave-roots", type=int, default=0, help="batched: camera paths per wave (0: autotuned)")
     ap.add_argument("--policy", default="smallest", choices=["smallest", "fifo", "share"],
@@ -372,6 +460,9 @@ def main():
         return
     if args.workload == "batched":
         bench_batched(args)
+        return
+    if args.workload == "served":
+        bench_served(args)
         return
 
     import torch

@@ -197,6 +197,7 @@ typedef struct MrtRenderStats {
 
 typedef struct MrtContext MrtContext;
 typedef struct MrtScene MrtScene;
+typedef struct MrtArena MrtArena;
 
 /* ---- context -------------------------------------------------------------------------------- */
 int mrt_context_create(int device, MrtContext **out);
@@ -206,10 +207,30 @@ int mrt_context_synchronize(MrtContext *ctx);
 /* Stream the context launches on (a cudaStream_t), for callers that order their own work. */
 void *mrt_context_stream(MrtContext *ctx);
 
+/* ---- device arena (no counterpart in the reference) ----------------------------------------- */
+/* One device allocation of `bytes` from which contexts that use it carve every scene buffer
+ * (geometry, trees, build scratch) and their render scratch: scenes come and go without cudaMalloc /
+ * cudaFree, so building or evicting a scene never synchronises the device while other work runs, and
+ * the sum of all resident scenes is bounded by the arena's size.  Several contexts on one device may
+ * share an arena (e.g. one building scenes while another renders); it is thread-safe.  Freeing a
+ * scene returns its blocks at once: destroy a scene only when no work that reads it is in flight. */
+int mrt_arena_create(int device, uint64_t bytes, MrtArena **out);
+/* MRT_ERR_STATE (and nothing freed) while buffers carved from the arena are alive. */
+int mrt_arena_destroy(MrtArena *arena);
+int mrt_arena_stats(MrtArena *arena, uint64_t *capacity, uint64_t *used, uint64_t *peak,
+                    uint64_t *largest_free);
+/* Later device allocations of ctx come from `arena` (NULL: cudaMalloc again); existing buffers keep
+ * their origin. */
+int mrt_context_set_arena(MrtContext *ctx, MrtArena *arena);
+
 /* ---- scene ---------------------------------------------------------------------------------- */
 int mrt_scene_create(MrtContext *ctx, const MrtSceneDesc *desc, MrtScene **out);
 void mrt_scene_destroy(MrtScene *scene);
 int mrt_scene_build(MrtScene *scene, const MrtAccelOpts *opts);
+/* Hand a scene to another context on the same device (e.g. from a context that builds scenes on one
+ * thread to the one that renders them); waits for the old context's work first.  No counterpart in
+ * the reference. */
+int mrt_scene_move(MrtScene *scene, MrtContext *ctx);
 /* Device bytes held by the scene (geometry + accelerator), for footprint admission. */
 uint64_t mrt_scene_device_bytes(const MrtScene *scene);
 /* Accelerator statistics: nodes (BVH records) or cells (grid), references, grid size. */

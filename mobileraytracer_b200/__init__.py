@@ -19,7 +19,7 @@ import numpy as np
 
 from . import capi
 
-__all__ = ["Context", "Scene", "Batch", "MrtError", "capi"]
+__all__ = ["Context", "Scene", "Batch", "Arena", "MrtError", "capi"]
 
 RAY_DTYPE = np.dtype([("origin", np.float32, 3), ("direction", np.float32, 3), ("depth", np.int32),
                       ("exclude", np.uint32)])
@@ -34,6 +34,14 @@ class MrtError(RuntimeError):
 
 def _is_torch_cuda(x) -> bool:
     return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+def _after_torch(ctx, *tensors):
+    """The library works on its own streams: make the context's stream wait for the work torch has
+    queued on its current stream (e.g. the zeroing or upload of a device buffer passed in)."""
+    if any(_is_torch_cuda(t) for t in tensors if t is not None):
+        import torch
+        torch.cuda.ExternalStream(ctx.stream).wait_stream(torch.cuda.current_stream())
 
 
 def _ptr(x):
@@ -57,6 +65,11 @@ class Context:
         self.device = device
         self._scenes = weakref.WeakSet()
         self._batches = weakref.WeakSet()
+
+    def set_arena(self, arena: "Arena | None"):
+        """Later device allocations of this context (scenes, their build scratch) come from `arena`."""
+        self.check(self.lib.mrt_context_set_arena(self.h, arena.h if arena is not None else None), "set_arena")
+        self._arena = arena
 
     def check(self, st: int, what: str):
         if st != capi.MRT_OK:
@@ -111,6 +124,14 @@ class Scene:
         self.ctx.check(self.lib.mrt_scene_build(self.h, ctypes.byref(o)), "mrt_scene_build")
         return self
 
+    def move_to(self, ctx: Context):
+        """Hand the scene to another context on the same device (mrt_scene_move)."""
+        ctx.check(self.lib.mrt_scene_move(self.h, ctx.h), "mrt_scene_move")
+        self.ctx._scenes.discard(self)
+        self.ctx = ctx
+        ctx._scenes.add(self)
+        return self
+
     def device_bytes(self) -> int:
         return int(self.lib.mrt_scene_device_bytes(self.h))
 
@@ -130,6 +151,7 @@ class Scene:
         rp, mem = _ptr(rays)
         hp, mem2 = _ptr(hits)
         assert mem == mem2, "rays and hits must both be host or both be device buffers"
+        _after_torch(self.ctx, rays, hits)
         self.ctx.check(self.lib.mrt_trace_closest(self.h, rp, n, hp, mem), "mrt_trace_closest")
         return hits
 
@@ -144,6 +166,7 @@ class Scene:
         rp, mem = _ptr(rays)
         dp, _ = _ptr(dist if _is_torch_cuda(dist) else np.ascontiguousarray(dist, np.float32))
         op, _ = _ptr(occluded)
+        _after_torch(self.ctx, rays, dist, occluded)
         self.ctx.check(self.lib.mrt_trace_any(self.h, rp, dp, n, op, mem), "mrt_trace_any")
         return occluded
 
@@ -171,6 +194,7 @@ class Scene:
             ap, mem2 = _ptr(accum)
             assert mem == mem2
         stats = capi.MrtRenderStats()
+        _after_torch(self.ctx, bitmap, accum)
         self.ctx.check(self.lib.mrt_render(self.h, ctypes.byref(camera), ctypes.byref(opts), bp, stride_bytes, ap, mem,
                                            ctypes.byref(stats)), "mrt_render")
         return bitmap, accum, stats
@@ -231,6 +255,7 @@ class Batch:
         j.stride_bytes = opts.width * 4 if stride_bytes is None else stride_bytes
         j.accum = accum.data_ptr() if accum is not None else None
         jid = ctypes.c_uint64()
+        _after_torch(self.ctx, bitmap, accum)
         self.ctx.check(self.lib.mrt_batch_submit(self.h, ctypes.byref(j), ctypes.byref(jid)), "mrt_batch_submit")
         self._keep[jid.value] = (scene, bitmap, accum)
         return jid.value
@@ -269,6 +294,38 @@ class Batch:
                 self.lib.mrt_batch_destroy(self.h)
             self.h = None
             self._keep = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Arena:
+    """One device allocation that scenes of the contexts using it are carved from (MrtArena)."""
+
+    def __init__(self, device: int, nbytes: int):
+        self.lib = capi.load()
+        h = ctypes.c_void_p()
+        st = self.lib.mrt_arena_create(device, int(nbytes), ctypes.byref(h))
+        if st != capi.MRT_OK:
+            raise MrtError(st, f"mrt_arena_create({nbytes} bytes on device {device}) failed")
+        self.h = h
+        self.device = device
+
+    def stats(self) -> dict:
+        v = [ctypes.c_uint64() for _ in range(4)]
+        self.lib.mrt_arena_stats(self.h, *[ctypes.byref(x) for x in v])
+        return {"capacity": v[0].value, "used": v[1].value, "peak": v[2].value, "largest_free": v[3].value}
+
+    def close(self):
+        """Frees the arena; raises while scenes carved from it are alive."""
+        if getattr(self, "h", None):
+            st = self.lib.mrt_arena_destroy(self.h)
+            if st != capi.MRT_OK:
+                raise MrtError(st, "mrt_arena_destroy: buffers carved from the arena are still alive")
+            self.h = None
 
     def __del__(self):
         try:

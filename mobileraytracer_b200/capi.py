@@ -156,6 +156,7 @@ def load() -> ctypes.CDLL:
         "mrt_scene_create": (ctypes.c_int, [vp, P(MrtSceneDesc), P(vp)]),
         "mrt_scene_destroy": (None, [vp]),
         "mrt_scene_build": (ctypes.c_int, [vp, P(MrtAccelOpts)]),
+        "mrt_scene_move": (ctypes.c_int, [vp, vp]),
         "mrt_scene_device_bytes": (ctypes.c_uint64, [vp]),
         "mrt_scene_accel_info": (ctypes.c_int, [vp, P(ctypes.c_uint64), P(ctypes.c_uint64), P(ctypes.c_int32)]),
         "mrt_trace_closest": (ctypes.c_int, [vp, vp, ctypes.c_uint32, vp, ctypes.c_uint32]),
@@ -172,6 +173,11 @@ def load() -> ctypes.CDLL:
         "mrt_batch_completed": (ctypes.c_int, [vp, P(ctypes.c_uint64), ctypes.c_uint32, P(ctypes.c_uint32)]),
         "mrt_batch_run": (ctypes.c_int, [vp]),
         "mrt_batch_stats": (ctypes.c_int, [vp, P(MrtBatchStats)]),
+        "mrt_arena_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, P(vp)]),
+        "mrt_arena_destroy": (ctypes.c_int, [vp]),
+        "mrt_arena_stats": (ctypes.c_int, [vp, P(ctypes.c_uint64), P(ctypes.c_uint64), P(ctypes.c_uint64),
+                                           P(ctypes.c_uint64)]),
+        "mrt_context_set_arena": (ctypes.c_int, [vp, vp]),
         "mrt_render_stop": (None, [vp]),
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
     }
@@ -189,4 +195,5 @@ EXPORTED_SYMBOLS = [
     "mrt_scene_accel_info", "mrt_trace_closest", "mrt_trace_any", "mrt_trace_closest_counts", "mrt_render",
     "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress", "mrt_batch_create", "mrt_batch_destroy",
     "mrt_batch_submit", "mrt_batch_step", "mrt_batch_completed", "mrt_batch_run", "mrt_batch_stats",
+    "mrt_arena_create", "mrt_arena_destroy", "mrt_arena_stats", "mrt_context_set_arena", "mrt_scene_move",
 ]

@@ -26,9 +26,76 @@ int cuda_status(MrtContext *ctx, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? MRT_ERR_OOM : MRT_ERR_CUDA;
 }
 
+static void arena_insert_free(MrtArena *a, size_t off, size_t size) {
+    // coalesce with the free neighbours
+    auto next = a->free_by_offset.lower_bound(off);
+    if (next != a->free_by_offset.end() && off + size == next->first) {
+        auto range = a->free_by_size.equal_range(next->second);
+        for (auto it = range.first; it != range.second; ++it)
+            if (it->second == next->first) { a->free_by_size.erase(it); break; }
+        size += next->second;
+        next = a->free_by_offset.erase(next);
+    }
+    if (next != a->free_by_offset.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            auto range = a->free_by_size.equal_range(prev->second);
+            for (auto it = range.first; it != range.second; ++it)
+                if (it->second == prev->first) { a->free_by_size.erase(it); break; }
+            off = prev->first;
+            size += prev->second;
+            a->free_by_offset.erase(prev);
+        }
+    }
+    a->free_by_offset[off] = size;
+    a->free_by_size.emplace(size, off);
+}
+
+static void *arena_alloc(MrtArena *a, size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    std::lock_guard<std::mutex> lock(a->mu);
+    auto it = a->free_by_size.lower_bound(bytes);   // best fit
+    if (it == a->free_by_size.end()) return nullptr;
+    const size_t size = it->first, off = it->second;
+    a->free_by_size.erase(it);
+    a->free_by_offset.erase(off);
+    if (size > bytes) {
+        a->free_by_offset[off + bytes] = size - bytes;
+        a->free_by_size.emplace(size - bytes, off + bytes);
+    }
+    a->used += bytes;
+    a->peak = std::max(a->peak, a->used);
+    ++a->live;
+    return a->base + off;
+}
+
+static void arena_free(MrtArena *a, void *p, size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    std::lock_guard<std::mutex> lock(a->mu);
+    arena_insert_free(a, (size_t)((char *)p - a->base), bytes);
+    a->used -= bytes;
+    --a->live;
+}
+
 int dev_alloc(MrtContext *ctx, DevBuf &b, size_t bytes) {
     dev_free(b);
     if (bytes == 0) bytes = 16;
+    if (ctx->arena) {
+        b.ptr = arena_alloc(ctx->arena, bytes);
+        if (!b.ptr) {
+            size_t largest = 0;
+            {
+                std::lock_guard<std::mutex> lock(ctx->arena->mu);
+                if (!ctx->arena->free_by_size.empty()) largest = ctx->arena->free_by_size.rbegin()->first;
+            }
+            set_error(ctx, "device arena: no free block of %zu bytes (used %zu of %zu, largest free block %zu)", bytes,
+                      ctx->arena->used, ctx->arena->capacity, largest);
+            return MRT_ERR_OOM;
+        }
+        b.bytes = bytes;
+        b.arena = ctx->arena;
+        return MRT_OK;
+    }
     const cudaError_t e = cudaMalloc(&b.ptr, bytes);
     if (e != cudaSuccess) {
         b.ptr = nullptr;
@@ -41,9 +108,13 @@ int dev_alloc(MrtContext *ctx, DevBuf &b, size_t bytes) {
 }
 
 void dev_free(DevBuf &b) {
-    if (b.ptr) cudaFree(b.ptr);
+    if (b.ptr) {
+        if (b.arena) arena_free(b.arena, b.ptr, b.bytes);
+        else cudaFree(b.ptr);
+    }
     b.ptr = nullptr;
     b.bytes = 0;
+    b.arena = nullptr;
 }
 
 int ensure(MrtContext *ctx, DevBuf &b, size_t bytes) {
@@ -149,6 +220,57 @@ void mrt_context_destroy(MrtContext *ctx) {
 }
 
 const char *mrt_context_error(const MrtContext *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int mrt_arena_create(int device, uint64_t bytes, MrtArena **out) {
+    if (!out || bytes == 0) return MRT_ERR_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return MRT_ERR_CUDA;
+    MrtArena *a = new (std::nothrow) MrtArena();
+    if (!a) return MRT_ERR_OOM;
+    a->device = device;
+    a->capacity = (size_t)(bytes & ~(uint64_t)255);
+    if (cudaMalloc(&a->base, a->capacity) != cudaSuccess) {
+        cudaGetLastError();
+        delete a;
+        return MRT_ERR_OOM;
+    }
+    a->free_by_offset[0] = a->capacity;
+    a->free_by_size.emplace(a->capacity, 0);
+    *out = a;
+    return MRT_OK;
+}
+
+int mrt_arena_destroy(MrtArena *a) {
+    if (!a) return MRT_OK;
+    {
+        std::lock_guard<std::mutex> lock(a->mu);
+        if (a->live) return MRT_ERR_STATE;   // buffers still carved from it
+    }
+    cudaSetDevice(a->device);
+    cudaFree(a->base);
+    delete a;
+    return MRT_OK;
+}
+
+int mrt_arena_stats(MrtArena *a, uint64_t *capacity, uint64_t *used, uint64_t *peak, uint64_t *largest_free) {
+    if (!a) return MRT_ERR_ARG;
+    std::lock_guard<std::mutex> lock(a->mu);
+    if (capacity) *capacity = a->capacity;
+    if (used) *used = a->used;
+    if (peak) *peak = a->peak;
+    if (largest_free) *largest_free = a->free_by_size.empty() ? 0 : a->free_by_size.rbegin()->first;
+    return MRT_OK;
+}
+
+int mrt_context_set_arena(MrtContext *ctx, MrtArena *arena) {
+    if (!ctx) return MRT_ERR_ARG;
+    if (arena && arena->device != ctx->device) {
+        set_error(ctx, "mrt_context_set_arena: arena on device %d, context on device %d", arena->device, ctx->device);
+        return MRT_ERR_ARG;
+    }
+    ctx->arena = arena;
+    return MRT_OK;
+}
 
 int mrt_context_synchronize(MrtContext *ctx) {
     if (!ctx) return MRT_ERR_ARG;
@@ -302,6 +424,20 @@ void mrt_scene_destroy(MrtScene *s) {
     cudaStreamSynchronize(s->ctx->stream);
     scene_free(s);
     delete s;
+}
+
+int mrt_scene_move(MrtScene *s, MrtContext *ctx) {
+    if (!s || !ctx) return MRT_ERR_ARG;
+    if (ctx->device != s->ctx->device) {
+        set_error(ctx, "mrt_scene_move: scene on device %d, context on device %d", s->ctx->device, ctx->device);
+        return MRT_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const int st = cuda_status(ctx, cudaStreamSynchronize(s->ctx->stream), "mrt_scene_move");
+    if (st != MRT_OK) return st;
+    s->ctx = ctx;
+    s->dev.error_flag = ctx->d_error;
+    return MRT_OK;
 }
 
 int mrt_scene_build(MrtScene *s, const MrtAccelOpts *o) {

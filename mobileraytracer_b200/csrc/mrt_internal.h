@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -12,9 +14,25 @@
 #include "../../include/mrt_cuda.h"
 #include "mrt_device.cuh"
 
+struct MrtArena;
+
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    MrtArena *arena = nullptr;   // carved from this arena (nullptr: cudaMalloc)
+};
+
+// One device allocation carved into the buffers of many scenes (geometry, trees, build scratch):
+// best-fit blocks of 256-byte granularity with coalescing on free.  Thread-safe; no CUDA call after
+// creation, so scene builds and evictions never synchronise the device.
+struct MrtArena {
+    int device = 0;
+    char *base = nullptr;
+    size_t capacity = 0;
+    std::mutex mu;
+    std::map<size_t, size_t> free_by_offset;          // offset -> size
+    std::multimap<size_t, size_t> free_by_size;       // size -> offset
+    size_t used = 0, peak = 0, live = 0;
 };
 
 struct MrtContext {
@@ -27,6 +45,7 @@ struct MrtContext {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];
+    MrtArena *arena = nullptr;          // device allocations of this context come from here when set
     // render scratch shared by the context's scenes (renders on one context are serialised on its
     // stream): wavefront queues, per-sample values, host-path bitmap staging
     DevBuf wave[8];
