@@ -10,7 +10,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libmrt_cuda.so")
+LIB_PATH = os.environ.get("MRT_CUDA_LIB") or os.path.join(HERE, "lib", "libmrt_cuda.so")
 
 MRT_OK, MRT_ERR_ARG, MRT_ERR_OOM, MRT_ERR_CUDA, MRT_ERR_LIMIT, MRT_ERR_CANCELLED, MRT_ERR_STATE = range(7)
 MRT_ACCEL_NAIVE, MRT_ACCEL_REGULAR_GRID, MRT_ACCEL_BVH = 0, 1, 2

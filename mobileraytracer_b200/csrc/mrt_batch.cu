@@ -179,7 +179,7 @@ struct BatchShadowWork {
 };
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_batch_extend(BatchState b, int level) {
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_extend(BatchState b, int level) {
     Level L = b.levels[level];
     L.start = min(L.start, b.ray_cap);
     L.count = min(L.count, b.ray_cap - L.start);
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_extend(BatchState b, int level
 }
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_batch_shadow(BatchState b, int level) {
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_shadow(BatchState b, int level) {
     const uint32_t n = min(b.levels[level].shadow_count, b.shadow_cap);
     BatchShadowWork work{b, n, b.work + 2 * level + 1};
     BatchLane lane;

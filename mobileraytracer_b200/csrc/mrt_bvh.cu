@@ -7,9 +7,12 @@
 // FAST tree: built on the device.  Triangle boxes padded outward -> 30-bit Morton codes of the
 // centroids -> stable LSD radix sort (own kernels) -> Karras' parallel hierarchy ("Maximizing
 // parallelism in the construction of BVHs, octrees and k-d trees", HPG 2012) -> bottom-up box fit
-// -> records in child-pair layout (32 bytes per record, the two children of a node adjacent so one
-// 64-byte fetch serves a traversal step), subtrees of <= kLeafMax triangles collapsed into leaves,
-// triangles copied in leaf order as 48-byte records.
+// -> records in child-pair layout (32 bytes per record), subtrees of <= kLeafMax triangles collapsed
+// into leaves -> the binary tree collapsed into kWide-wide nodes (one 128-byte node = the kWide
+// child records a traversal step tests; each wide node opens the largest internal children of a
+// binary node until it is full), wide nodes numbered level by level -> triangles copied in leaf
+// order as 48-byte records.  A traversal step of the wide tree replaces about two of the binary
+// tree's, halving the chain of dependent node fetches per ray.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -364,6 +367,79 @@ __global__ void k_single_leaf(const float4 *bmin, const float4 *bmax, float4 *re
     write_record(records, bmin[0], bmax[0], 0u, 1u);
 }
 
+// ------------------------------ binary -> wide collapse ---------------------------------------
+struct CollapseItem {
+    uint32_t bin;    // binary internal node (children at records 2 + 2 bin, 3 + 2 bin)
+    uint32_t wide;   // wide node it becomes
+};
+
+__device__ __forceinline__ float half_area(float4 lo, float4 hi) {
+    const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ void write_empty_slot(float4 *rec) {
+    rec[0] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+    rec[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+}
+
+// the root: a leaf root becomes slot 0 of wide node 0; an internal root is the first item
+__global__ void k_collapse_root(const float4 *bin, float4 *wide, CollapseItem *queue, uint32_t *ctrs) {
+    const float4 lo = bin[0], hi = bin[1];
+    if (__float_as_int(hi.w) > 0) {
+        write_record(wide, lo, hi, __float_as_uint(lo.w), (uint32_t)__float_as_int(hi.w));
+        for (int k = 1; k < kWide; ++k) write_empty_slot(wide + 2 * k);
+        ctrs[0] = 0;   // next level: empty
+    } else {
+        queue[0] = CollapseItem{0u, 0u};
+        ctrs[0] = 1;
+    }
+    ctrs[1] = 1;       // wide nodes allocated
+}
+
+// one level: every item's binary node becomes a wide node; its internal slots get wide nodes of
+// the next level.  ctrs[0]: items of the next level, ctrs[1]: wide nodes, ctrs[2]: error
+__global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, const CollapseItem *__restrict__ in,
+                           uint32_t n_in, CollapseItem *out, uint32_t cap, float4 *wide, uint32_t *ctrs) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_in) return;
+    const CollapseItem it = in[i];
+    uint32_t rec[kWide];
+    int m = 2;
+    rec[0] = 2u + 2u * it.bin;
+    rec[1] = rec[0] + 1u;
+    if ((uint64_t)rec[1] >= n_records) { atomicMax(&ctrs[2], 1u); return; }
+    for (;;) {   // open the internal slot with the largest box while there is room
+        if (m >= kWide) break;
+        int best = -1;
+        float best_area = -1.0f;
+        for (int k = 0; k < m; ++k) {
+            const float4 lo = bin[2 * (size_t)rec[k]], hi = bin[2 * (size_t)rec[k] + 1];
+            if (__float_as_int(hi.w) != 0) continue;
+            const float a = half_area(lo, hi);
+            if (a > best_area) { best_area = a; best = k; }
+        }
+        if (best < 0) break;
+        const uint32_t a = __float_as_uint(bin[2 * (size_t)rec[best]].w);
+        if ((uint64_t)a + 1u >= n_records) { atomicMax(&ctrs[2], 1u); return; }
+        rec[best] = a;
+        rec[m++] = a + 1u;
+    }
+    float4 *node = wide + (size_t)it.wide * (2 * kWide);
+    for (int k = 0; k < kWide; ++k) {
+        if (k >= m) { write_empty_slot(node + 2 * k); continue; }
+        const float4 lo = bin[2 * (size_t)rec[k]], hi = bin[2 * (size_t)rec[k] + 1];
+        const int b = __float_as_int(hi.w);
+        if (b > 0) { write_record(node + 2 * k, lo, hi, __float_as_uint(lo.w), (uint32_t)b); continue; }
+        const uint32_t a = __float_as_uint(lo.w);
+        const uint32_t j = atomicAdd(&ctrs[1], 1u);
+        const uint32_t q = atomicAdd(&ctrs[0], 1u);
+        if (j >= cap || q >= cap || a < 2u) { atomicMax(&ctrs[2], 1u); write_empty_slot(node + 2 * k); continue; }
+        out[q] = CollapseItem{(a - 2u) / 2u, j};
+        write_record(node + 2 * k, lo, hi, j, 0u);
+    }
+}
+
 }  // namespace
 
 namespace mrt_host {
@@ -388,6 +464,10 @@ int build_fast_bvh(MrtScene *s) {
         s->dev.fnodes = nullptr;
         s->dev.ftris = nullptr;
         return MRT_OK;
+    }
+    if (n >= kMaxLeafFirst) {
+        set_error(ctx, "fast bvh: at most %u triangles", kMaxLeafFirst - 1u);
+        return MRT_ERR_ARG;
     }
     int st = MRT_OK;
     const uint64_t n_records = 2ull + 2ull * (n > 1 ? n - 1 : 0) + 2ull;
@@ -449,8 +529,52 @@ int build_fast_bvh(MrtScene *s) {
                      &pint, &pleaf, &ctr, &imin, &imax};
     for (DevBuf *b : tmp) dev_free(*b);
     if (st != MRT_OK) return st;
-    s->fnode_count = n_records;
-    s->dev.n_fnodes = (uint32_t)n_records;
+    // collapse into wide nodes, level by level
+    DevBuf wide, queue[2], wctr;
+    const uint32_t cap = n;   // wide nodes <= binary internal nodes + 1
+    A(wide, 32ull * kWide * cap);
+    A(queue[0], sizeof(CollapseItem) * cap);
+    A(queue[1], sizeof(CollapseItem) * cap);
+    A(wctr, 16);
+    uint32_t h[3] = {0, 0, 0};
+    if (st == MRT_OK) {
+        cudaMemsetAsync(wctr.ptr, 0, 16, q);
+        k_collapse_root<<<1, 1, 0, q>>>((const float4 *)s->fnodes.ptr, (float4 *)wide.ptr, (CollapseItem *)queue[0].ptr,
+                                        (uint32_t *)wctr.ptr);
+        st = cuda_status(ctx, cudaMemcpyAsync(h, wctr.ptr, 12, cudaMemcpyDeviceToHost, q), "collapse");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse");
+    }
+    int cur_q = 0;
+    for (int level = 0; st == MRT_OK && h[0] > 0 && h[2] == 0; ++level) {
+        if (level > 4096) { st = MRT_ERR_LIMIT; break; }
+        const uint32_t n_in = h[0];
+        cudaMemsetAsync(wctr.ptr, 0, 4, q);
+        k_collapse<<<(n_in + 127) / 128, 128, 0, q>>>((const float4 *)s->fnodes.ptr, (uint32_t)n_records,
+                                                       (const CollapseItem *)queue[cur_q].ptr, n_in,
+                                                       (CollapseItem *)queue[1 - cur_q].ptr, cap, (float4 *)wide.ptr,
+                                                       (uint32_t *)wctr.ptr);
+        cur_q = 1 - cur_q;
+        st = cuda_status(ctx, cudaMemcpyAsync(h, wctr.ptr, 12, cudaMemcpyDeviceToHost, q), "collapse");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse");
+    }
+    if (st == MRT_OK && h[2] != 0) {
+        set_error(ctx, "fast bvh: inconsistent binary tree while collapsing");
+        st = MRT_ERR_LIMIT;
+    }
+    const uint64_t n_wide = h[1];
+    if (st == MRT_OK) {   // exact-size copy; the binary records and the scratch go
+        dev_free(s->fnodes);
+        st = dev_alloc(ctx, s->fnodes, 32ull * kWide * n_wide);
+        if (st == MRT_OK)
+            st = cuda_status(ctx, cudaMemcpyAsync(s->fnodes.ptr, wide.ptr, 32ull * kWide * n_wide,
+                                                  cudaMemcpyDeviceToDevice, q), "collapse copy");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse copy");
+    }
+    DevBuf *tmp2[] = {&wide, &queue[0], &queue[1], &wctr};
+    for (DevBuf *b : tmp2) dev_free(*b);
+    if (st != MRT_OK) return st;
+    s->fnode_count = n_wide * kWide;
+    s->dev.n_fnodes = (uint32_t)(n_wide * kWide);
     s->dev.fnodes = (const float4 *)s->fnodes.ptr;
     s->dev.ftris = (const float4 *)s->ftris.ptr;
     return MRT_OK;

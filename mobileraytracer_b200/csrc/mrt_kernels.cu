@@ -43,22 +43,6 @@ __global__ void __launch_bounds__(128) k_trace_any(DevScene s, const MrtRay *ray
     }
 }
 
-// counting replay of the FAST traversal: per ray, node records and triangle records fetched
-__global__ void __launch_bounds__(128) k_trace_counts(DevScene s, const MrtRay *rays, uint32_t n, uint32_t *nodes,
-                                                      uint32_t *tris) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const Ray r = load_ray(rays, i);
-        float len = kRayLengthMax;
-        uint32_t id = MRT_HIT_NONE;
-        naive_trace<kPlane>(s, r, len, id);
-        naive_trace<kSphere>(s, r, len, id);
-        FastCounts c{0, 0};
-        fast_trace<true>(s, r, len, id, &c);
-        nodes[i] = c.nodes;
-        tris[i] = c.tris;
-    }
-}
-
 // persistent FAST-BVH versions: work items are rays of the input array
 struct TraceLane {
     uint32_t i;
@@ -114,13 +98,13 @@ struct AnyWork {
     __device__ void finish(TraceLane &lane, bool occluded) const { occ[lane.i] = occluded ? 1 : 0; }
 };
 
-__global__ void __launch_bounds__(128) k_trace_any_persistent(DevScene s, AnyWork work) {
+__global__ void __launch_bounds__(128, 8) k_trace_any_persistent(DevScene s, AnyWork work) {
     TraceLane lane;
     persistent_any(s, work, lane);
 }
 
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_trace_persistent(DevScene s, TraceWork<kCount> work) {
+__global__ void __launch_bounds__(128, 8) k_trace_persistent(DevScene s, TraceWork<kCount> work) {
     TraceLane lane;
     persistent_closest<kCount>(s, work, lane);
 }

@@ -19,15 +19,12 @@
 
 namespace mrt {
 
-constexpr uint32_t kPairNone = 0xFFFFFFFFu;
-
 struct FastTrav {
     FastRay f;
     float best_t;
     uint32_t best_i;
-    uint32_t pair;          // child pair to expand next (kPairNone: pop the stack)
-    uint32_t leaf0_first, leaf0_count, leaf1_first, leaf1_count;   // pending leaves (named: stay in registers)
-    int n_leaf;
+    uint32_t node;          // node to expand next (kNodeNone: pop the stack)
+    uint32_t leaf_first, leaf_count;   // pending leaf (count 0: none)
     int sp;
     bool have;
     uint32_t c_nodes, c_tris;
@@ -45,90 +42,61 @@ __device__ __forceinline__ void trav_begin(const DevScene &s, const Ray &r, floa
     t.best_t = len0;
     t.best_i = 0;
     t.have = false;
-    t.pair = kPairNone;
-    t.n_leaf = 0;
+    t.node = s.n_tri == 0 ? kNodeNone : 0u;   // the root node
+    t.leaf_count = 0;
     t.sp = 0;
     t.c_nodes = 0;
     t.c_tris = 0;
-    if (s.n_tri == 0) return;
-    const float4 lo = __ldg(&s.fnodes[0]), hi = __ldg(&s.fnodes[1]);
-    if (kCount) t.c_nodes++;
-    float tn;
-    if (!fast_slab(lo, hi, t.f, t.best_t, tn)) return;
-    const int b = __float_as_int(hi.w);
-    if (b > 0) {
-        t.leaf0_first = (uint32_t)__float_as_int(lo.w);
-        t.leaf0_count = (uint32_t)b;
-        t.n_leaf = 1;
-    } else {
-        t.pair = (uint32_t)__float_as_int(lo.w);
-    }
 }
 
 __device__ __forceinline__ bool trav_wants_node(const FastTrav &t) {
-    return t.n_leaf == 0 && (t.pair != kPairNone || t.sp > 0);
+    return t.leaf_count == 0 && (t.node != kNodeNone || t.sp > 0);
 }
 __device__ __forceinline__ bool trav_finished(const FastTrav &t) {
-    return t.n_leaf == 0 && t.pair == kPairNone && t.sp == 0;
+    return t.leaf_count == 0 && t.node == kNodeNone && t.sp == 0;
 }
 
-// one node step: pop (with distance culling) or expand the current pair
+__device__ __forceinline__ void trav_take(FastTrav &t, uint32_t code) {
+    if (code & kLeafCode) {
+        t.leaf_first = code_first(code);
+        t.leaf_count = code_count(code);
+        t.node = kNodeNone;
+    } else {
+        t.node = code;
+    }
+}
+
+// one node step: expand the current node (popping one first, with distance culling, when there is
+// none), nearest child next and the other hits pushed far to near
 template <bool kCount, class S>
 __device__ __forceinline__ void trav_node_step(const S &s, FastTrav &t, TravStack &st) {
-    if (t.pair == kPairNone) {
+    if (t.node == kNodeNone) {
         while (t.sp > 0) {
             --t.sp;
-            if (st.t[t.sp] <= t.best_t * 1.000001f) { t.pair = st.n[t.sp]; break; }
+            if (st.t[t.sp] <= t.best_t * 1.000001f) { trav_take(t, st.n[t.sp]); break; }
         }
-        return;
+        if (t.node == kNodeNone) return;   // a leaf, or nothing left
     }
-    const uint32_t pair = t.pair;
-    if (pair + 1 >= s.n_fnodes) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
-    const float4 *p = s.fnodes + 2 * pair;
-    const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-    if (kCount) t.c_nodes += 2;
-    float tl, tr;
-    const bool hl = fast_slab(l0, l1, t.f, t.best_t, tl);
-    const bool hr = fast_slab(r0, r1, t.f, t.best_t, tr);
-    const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
-    // leaves first, nearer one first
-    const bool ll = hl && lb > 0, rl = hr && rb > 0;
-    const bool swap = ll && rl && tr < tl;
-    const uint32_t lf = (uint32_t)__float_as_int(l0.w), rf = (uint32_t)__float_as_int(r0.w);
-    if (ll && rl) {
-        t.leaf0_first = swap ? rf : lf; t.leaf0_count = (uint32_t)(swap ? rb : lb);
-        t.leaf1_first = swap ? lf : rf; t.leaf1_count = (uint32_t)(swap ? lb : rb);
-        t.n_leaf = 2;
-    } else if (ll || rl) {
-        t.leaf0_first = ll ? lf : rf; t.leaf0_count = (uint32_t)(ll ? lb : rb);
-        t.n_leaf = 1;
-    } else {
-        t.n_leaf = 0;
-    }
-    const bool il = hl && lb == 0, ir = hr && rb == 0;
-    if (il && ir) {
-        const bool left_first = tl <= tr;
-        if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
-        st.n[t.sp] = (uint32_t)__float_as_int(left_first ? r0.w : l0.w);
-        st.t[t.sp] = left_first ? tr : tl;
-        ++t.sp;
-        t.pair = (uint32_t)__float_as_int(left_first ? l0.w : r0.w);
-    } else if (il) {
-        t.pair = (uint32_t)__float_as_int(l0.w);
-    } else if (ir) {
-        t.pair = (uint32_t)__float_as_int(r0.w);
-    } else {
-        t.pair = kPairNone;
-    }
+    if (!node_in_range(s, t.node)) { raise_error(s, MRT_ERR_LIMIT); t.node = kNodeNone; t.sp = 0; return; }
+    float ct[kWide];
+    uint32_t cc[kWide];
+    const int n = wide_children<true>(s, t.node, t.f, t.best_t, ct, cc);
+    if (kCount) t.c_nodes += kWide;
+    t.node = kNodeNone;
+    if (n == 0) return;
+    if (t.sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.sp = 0; return; }
+#pragma unroll
+    for (int k = kWide - 1; k >= 1; --k)
+        if (k < n) { st.n[t.sp] = cc[k]; st.t[t.sp] = ct[k]; ++t.sp; }
+    trav_take(t, cc[0]);
 }
 
 template <bool kCount, class S>
 __device__ __forceinline__ void trav_leaf_step(const S &s, const Ray &r, FastTrav &t) {
     FastCounts cnt{0, 0};
-    fast_leaf<kCount>(s, r, t.leaf0_first, t.leaf0_count, t.best_t, t.best_i, t.have, cnt);
-    if (t.n_leaf > 1) fast_leaf<kCount>(s, r, t.leaf1_first, t.leaf1_count, t.best_t, t.best_i, t.have, cnt);
+    fast_leaf<kCount>(s, r, t.leaf_first, t.leaf_count, t.best_t, t.best_i, t.have, cnt);
     if (kCount) t.c_tris += cnt.tris;
-    t.n_leaf = 0;
+    t.leaf_count = 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -193,7 +161,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             if (w) trav_node_step<kCount>(work.view(lane, s), t, stk);
         }
         // 3. leaf phase
-        if (active && t.n_leaf > 0) trav_leaf_step<kCount>(work.view(lane, s), r, t);
+        if (active && t.leaf_count > 0) trav_leaf_step<kCount>(work.view(lane, s), r, t);
         // 4. completion
         if (active && trav_finished(t)) {
             float len = len0;
@@ -219,94 +187,71 @@ namespace mrt {
 struct OccTrav {
     FastRay f;
     float dist;
-    uint32_t pair;
-    uint32_t leaf0_first, leaf0_count, leaf1_first, leaf1_count;
-    int n_leaf;
+    uint32_t node;
+    uint32_t leaf_first, leaf_count;
     int sp;
     bool occluded;
 };
 
 __device__ __forceinline__ void occ_begin(const DevScene &s, const Ray &r, float dist, OccTrav &t) {
     t.dist = dist;
-    t.pair = kPairNone;
-    t.n_leaf = 0;
+    t.node = kNodeNone;
+    t.leaf_count = 0;
     t.sp = 0;
     t.occluded = naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist);
     if (t.occluded || s.n_tri == 0) return;
     t.f = fast_ray(r);
-    const float4 lo = __ldg(&s.fnodes[0]), hi = __ldg(&s.fnodes[1]);
-    float tn;
-    if (!fast_slab(lo, hi, t.f, dist, tn)) return;
-    const int b = __float_as_int(hi.w);
-    if (b > 0) {
-        t.leaf0_first = (uint32_t)__float_as_int(lo.w);
-        t.leaf0_count = (uint32_t)b;
-        t.n_leaf = 1;
-    } else {
-        t.pair = (uint32_t)__float_as_int(lo.w);
-    }
+    t.node = 0u;
 }
 
 __device__ __forceinline__ bool occ_wants_node(const OccTrav &t) {
-    return !t.occluded && t.n_leaf == 0 && (t.pair != kPairNone || t.sp > 0);
+    return !t.occluded && t.leaf_count == 0 && (t.node != kNodeNone || t.sp > 0);
 }
 __device__ __forceinline__ bool occ_finished(const OccTrav &t) {
-    return t.occluded || (t.n_leaf == 0 && t.pair == kPairNone && t.sp == 0);
+    return t.occluded || (t.leaf_count == 0 && t.node == kNodeNone && t.sp == 0);
+}
+
+__device__ __forceinline__ void occ_take(OccTrav &t, uint32_t code) {
+    if (code & kLeafCode) {
+        t.leaf_first = code_first(code);
+        t.leaf_count = code_count(code);
+        t.node = kNodeNone;
+    } else {
+        t.node = code;
+    }
 }
 
 template <class S>
 __device__ __forceinline__ void occ_node_step(const S &s, OccTrav &t, uint32_t *stack_n) {
-    if (t.pair == kPairNone) {
-        if (t.sp > 0) t.pair = stack_n[--t.sp];
-        return;
+    if (t.node == kNodeNone) {
+        if (t.sp > 0) occ_take(t, stack_n[--t.sp]);
+        if (t.node == kNodeNone) return;   // a leaf, or nothing left
     }
-    const uint32_t pair = t.pair;
-    if (pair + 1 >= s.n_fnodes) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
-    const float4 *p = s.fnodes + 2 * pair;
-    const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-    float tl, tr;
-    const bool hl = fast_slab(l0, l1, t.f, t.dist, tl);
-    const bool hr = fast_slab(r0, r1, t.f, t.dist, tr);
-    const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
-    const bool ll = hl && lb > 0, rl = hr && rb > 0;
-    const uint32_t lf = (uint32_t)__float_as_int(l0.w), rf = (uint32_t)__float_as_int(r0.w);
-    if (ll && rl) {
-        t.leaf0_first = lf; t.leaf0_count = (uint32_t)lb; t.leaf1_first = rf; t.leaf1_count = (uint32_t)rb;
-        t.n_leaf = 2;
-    } else if (ll || rl) {
-        t.leaf0_first = ll ? lf : rf; t.leaf0_count = (uint32_t)(ll ? lb : rb);
-        t.n_leaf = 1;
-    } else {
-        t.n_leaf = 0;
-    }
-    const bool il = hl && lb == 0, ir = hr && rb == 0;
-    if (il && ir) {
-        if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.pair = kPairNone; t.sp = 0; return; }
-        stack_n[t.sp++] = (uint32_t)__float_as_int(r0.w);
-        t.pair = (uint32_t)__float_as_int(l0.w);
-    } else if (il) {
-        t.pair = (uint32_t)__float_as_int(l0.w);
-    } else if (ir) {
-        t.pair = (uint32_t)__float_as_int(r0.w);
-    } else {
-        t.pair = kPairNone;
-    }
+    if (!node_in_range(s, t.node)) { raise_error(s, MRT_ERR_LIMIT); t.node = kNodeNone; t.sp = 0; return; }
+    float ct[kWide];
+    uint32_t cc[kWide];
+    const int n = wide_children<false>(s, t.node, t.f, t.dist, ct, cc);
+    t.node = kNodeNone;
+    if (n == 0) return;
+    if (t.sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.sp = 0; return; }
+#pragma unroll
+    for (int k = kWide - 1; k >= 1; --k)
+        if (k < n) stack_n[t.sp++] = cc[k];
+    occ_take(t, cc[0]);
 }
 
 template <class S>
 __device__ __forceinline__ void occ_leaf_step(const S &s, const Ray &r, OccTrav &t) {
-    for (int q = 0; q < t.n_leaf && !t.occluded; ++q) {
-        const uint32_t first = q == 0 ? t.leaf0_first : t.leaf1_first, count = q == 0 ? t.leaf0_count : t.leaf1_count;
-        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
-        for (uint32_t k = first; k < first + count; ++k) {
-            const float4 A = __ldg(&s.ftris[3 * k]);
-            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
-            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
-            if (tri_occ(v3(A), v3(AB), v3(AC), r, t.dist)) { t.occluded = true; break; }
-        }
+    const uint32_t first = t.leaf_first, count = t.leaf_count;
+    t.leaf_count = 0;
+    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
+    for (uint32_t k = first; k < first + count; ++k) {
+        const float4 A = __ldg(&s.ftris[3 * k]);
+        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
+        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+        if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
+        if (tri_occ(v3(A), v3(AB), v3(AC), r, t.dist)) { t.occluded = true; return; }
     }
-    t.n_leaf = 0;
 }
 
 template <class Work, class Lane>
@@ -345,7 +290,7 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
             if (!__any_sync(FULL, w)) break;
             if (w) occ_node_step(work.view(lane, s), t, stack_n);
         }
-        if (active && t.n_leaf > 0) occ_leaf_step(work.view(lane, s), r, t);
+        if (active && t.leaf_count > 0) occ_leaf_step(work.view(lane, s), r, t);
         if (active && occ_finished(t)) {
             work.finish(lane, t.occluded);
             active = false;

@@ -125,7 +125,7 @@ struct NsWork {
     }
 };
 
-__global__ void __launch_bounds__(128) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
+__global__ void __launch_bounds__(128, 8) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
                                                                uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
@@ -274,7 +274,7 @@ struct ShadowWork {
     }
 };
 
-__global__ void __launch_bounds__(128) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+__global__ void __launch_bounds__(128, 8) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const Level L = clamp_level(w, w.levels[level]);
     ExtendWork work{w, L, ctr};
     WaveLane lane;
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128) k_wave_extend_fast(DevScene s, WaveState 
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
-__global__ void __launch_bounds__(128) k_wave_shadow_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+__global__ void __launch_bounds__(128, 8) k_wave_shadow_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const uint32_t n = min(w.levels[level].shadow_count, w.shadow_cap);
     ShadowWork work{w, n, ctr};
     WaveLane lane;

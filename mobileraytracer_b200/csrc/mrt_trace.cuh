@@ -6,15 +6,16 @@
 // keep that order and those comparisons:
 //   * NAIVE, REGULAR_GRID and BVH/REFERENCE walk the reference structures in the reference order
 //     with the reference box test, so the result is the reference's bit for bit;
-//   * BVH/FAST walks a Morton-ordered tree front to back with a conservative box test and keeps the
-//     lexicographic minimum (t, index): the Naive<T> result without visiting every triangle.
+//   * BVH/FAST walks a 4-wide tree (a Morton-ordered binary tree collapsed on the device) front to
+//     back with a conservative box test and keeps the lexicographic minimum (t, index): the
+//     Naive<T> result without visiting every triangle.
 #pragma once
 
 #include "mrt_device.cuh"
 
 namespace mrt {
 
-constexpr int kFastStack = 64;
+constexpr int kFastStack = 128;           // entries of the FAST traversal stack (3 pushes per node at most)
 constexpr int kRefStack = 128;
 constexpr uint32_t kMaxGridSteps = 1u << 20;
 constexpr uint32_t kMaxBvhSteps = 1u << 24;   // traversal iterations per ray before MRT_ERR_LIMIT
@@ -334,26 +335,41 @@ __device__ bool grid_occ(const DevScene &s, const Ray &r, float dist) {
 // order as 48-byte records.  Conservative slab test against padded boxes; front-to-back order
 // with the entry distance kept on the stack.
 // ---------------------------------------------------------------------------------------------
+// A ray prepared for the conservative box test of the FAST tree.  The plane distances are computed
+// as fma(plane, inv, -c) with c = o * inv moved outward by a margin (2^-20 |o * inv|, more than the
+// rounding of o * inv and of the shift itself), so the entry distance is never overestimated and the
+// exit distance never underestimated; the remaining rounding is relative and covered by the 1e-6
+// tolerance of the comparison.  The test may therefore accept a box the ray misses, never reject one
+// it touches.
 struct FastRay {
-    V3 o, inv;
+    V3 inv;
+    V3 clo, chi;   // offsets of the lo and hi planes
 };
+
+__device__ __forceinline__ float fast_shift(float p, bool up) {
+    const float m = fabsf(p) * 0x1p-20f;
+    return up ? p + m : p - m;
+}
 
 __device__ __forceinline__ FastRay fast_ray(const Ray &r) {
     FastRay f;
-    f.o = r.o;
     const float e = 1e-20f;
     const float dx = fabsf(r.d.x) < e ? copysignf(e, r.d.x) : r.d.x;
     const float dy = fabsf(r.d.y) < e ? copysignf(e, r.d.y) : r.d.y;
     const float dz = fabsf(r.d.z) < e ? copysignf(e, r.d.z) : r.d.z;
     f.inv = V3{1.0f / dx, 1.0f / dy, 1.0f / dz};
+    const float px = r.o.x * f.inv.x, py = r.o.y * f.inv.y, pz = r.o.z * f.inv.z;
+    // the lo plane is the entry plane when inv >= 0: its offset moves up (distance down)
+    f.clo = V3{fast_shift(px, f.inv.x >= 0.0f), fast_shift(py, f.inv.y >= 0.0f), fast_shift(pz, f.inv.z >= 0.0f)};
+    f.chi = V3{fast_shift(px, f.inv.x < 0.0f), fast_shift(py, f.inv.y < 0.0f), fast_shift(pz, f.inv.z < 0.0f)};
     return f;
 }
 
-// true when the ray segment [0, tmax] may touch the box; tnear = entry distance
+// true when the ray segment [0, tmax] may touch the box; tnear = entry distance (a lower bound)
 __device__ __forceinline__ bool fast_slab(float4 lo, float4 hi, const FastRay &f, float tmax, float &tnear) {
-    const float x1 = (lo.x - f.o.x) * f.inv.x, x2 = (hi.x - f.o.x) * f.inv.x;
-    const float y1 = (lo.y - f.o.y) * f.inv.y, y2 = (hi.y - f.o.y) * f.inv.y;
-    const float z1 = (lo.z - f.o.z) * f.inv.z, z2 = (hi.z - f.o.z) * f.inv.z;
+    const float x1 = __fmaf_rn(lo.x, f.inv.x, -f.clo.x), x2 = __fmaf_rn(hi.x, f.inv.x, -f.chi.x);
+    const float y1 = __fmaf_rn(lo.y, f.inv.y, -f.clo.y), y2 = __fmaf_rn(hi.y, f.inv.y, -f.chi.y);
+    const float z1 = __fmaf_rn(lo.z, f.inv.z, -f.clo.z), z2 = __fmaf_rn(hi.z, f.inv.z, -f.chi.z);
     const float tn = fmaxf(fmaxf(fminf(x1, x2), fminf(y1, y2)), fmaxf(fminf(z1, z2), 0.0f));
     const float tf = fminf(fminf(fmaxf(x1, x2), fmaxf(y1, y2)), fminf(fmaxf(z1, z2), tmax));
     tnear = tn;
@@ -386,7 +402,74 @@ __device__ __forceinline__ void fast_leaf(const S &s, const Ray &r, uint32_t fir
     }
 }
 
-// closest triangle with the reference's accept rule against the incoming length `len`
+__device__ __forceinline__ uint32_t leaf_code(uint32_t first, uint32_t count) {
+    return kLeafCode | ((count - 1u) << 27) | first;
+}
+__device__ __forceinline__ uint32_t code_first(uint32_t c) { return c & (kMaxLeafFirst - 1u); }
+__device__ __forceinline__ uint32_t code_count(uint32_t c) { return ((c >> 27) & 15u) + 1u; }
+
+__device__ __forceinline__ void cmp_swap(float (&t)[kWide], uint32_t (&c)[kWide], int i, int j) {
+    const bool sw = t[j] < t[i];
+    const float ti = t[i], tj = t[j];
+    const uint32_t ci = c[i], cj = c[j];
+    t[i] = sw ? tj : ti;
+    t[j] = sw ? ti : tj;
+    c[i] = sw ? cj : ci;
+    c[j] = sw ? ci : cj;
+}
+
+// One node of the FAST tree: kWide child records {min.xyz, a}{max.xyz, b} (b = 0: internal child,
+// node a; b > 0: leaf of b triangles at a; b < 0: empty slot).  Returns the number of children the
+// ray segment [0, tmax] may touch; with kSort their (entry distance, code) come first, nearest
+// first, the others follow at +inf.
+template <bool kSort, class S>
+__device__ __forceinline__ int wide_children(const S &s, uint32_t node, const FastRay &f, float tmax,
+                                             float (&t)[kWide], uint32_t (&c)[kWide]) {
+    const float4 *p = s.fnodes + (size_t)node * (2 * kWide);
+    float4 lo[kWide], hi[kWide];
+#pragma unroll
+    for (int k = 0; k < kWide; ++k) {
+        lo[k] = __ldg(p + 2 * k);
+        hi[k] = __ldg(p + 2 * k + 1);
+    }
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < kWide; ++k) {
+        const int b = __float_as_int(hi[k].w);
+        float tn;
+        const bool hit = fast_slab(lo[k], hi[k], f, tmax, tn) && b >= 0;
+        t[k] = hit ? tn : __int_as_float(0x7f800000);
+        c[k] = b > 0 ? leaf_code(__float_as_uint(lo[k].w), (uint32_t)b) : __float_as_uint(lo[k].w);
+        n += hit ? 1 : 0;
+    }
+    if (kSort) {
+        static_assert(kWide == 4, "sorting network for 4 children");
+        cmp_swap(t, c, 0, 1);
+        cmp_swap(t, c, 2, 3);
+        cmp_swap(t, c, 0, 2);
+        cmp_swap(t, c, 1, 3);
+        cmp_swap(t, c, 1, 2);
+    } else {
+        // compact the hits to the front, order kept
+#pragma unroll
+        for (int k = 1; k < kWide; ++k)
+#pragma unroll
+            for (int m = k; m > 0; --m)
+                if (t[m - 1] == __int_as_float(0x7f800000) && t[m] != __int_as_float(0x7f800000)) {
+                    t[m - 1] = t[m]; t[m] = __int_as_float(0x7f800000);
+                    const uint32_t x = c[m - 1]; c[m - 1] = c[m]; c[m] = x;
+                }
+    }
+    return n;
+}
+
+template <class S>
+__device__ __forceinline__ bool node_in_range(const S &s, uint32_t node) {
+    return (uint64_t)(node + 1u) * kWide <= (uint64_t)s.n_fnodes;
+}
+
+// closest triangle with the reference's accept rule against the incoming length `len`: front to
+// back, leaves as they are reached, entries beyond the best distance culled when popped
 template <bool kCount = false>
 __device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t &id, FastCounts *counts = nullptr) {
     if (s.n_tri == 0) return false;
@@ -395,57 +478,35 @@ __device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t
     float best_t = len;
     uint32_t best_i = 0;   // ties with a plane/sphere distance never win (index < 0 is impossible)
     bool have = false;
-    const float4 root_lo = __ldg(&s.fnodes[0]), root_hi = __ldg(&s.fnodes[1]);
-    if (kCount) cnt.nodes++;
-    float tn;
-    const int root_b = __float_as_int(root_hi.w);
-    if (fast_slab(root_lo, root_hi, f, best_t, tn)) {
-        if (root_b > 0) {
-            fast_leaf<kCount>(s, r, (uint32_t)__float_as_int(root_lo.w), (uint32_t)root_b, best_t, best_i, have, cnt);
+    uint32_t stack_n[kFastStack];
+    float stack_t[kFastStack];
+    int sp = 0;
+    uint32_t cur = 0;      // the root node
+    uint32_t steps = 0;
+    for (;;) {
+        if (cur == kNodeNone) {
+            bool found = false;
+            while (sp > 0) {
+                --sp;
+                if (stack_t[sp] <= best_t * 1.000001f) { cur = stack_n[sp]; found = true; break; }
+            }
+            if (!found) break;
+        } else if (cur & kLeafCode) {
+            fast_leaf<kCount>(s, r, code_first(cur), code_count(cur), best_t, best_i, have, cnt);
+            cur = kNodeNone;
         } else {
-            uint32_t stack_n[kFastStack];
-            float stack_t[kFastStack];
-            int sp = 0;
-            uint32_t pair = (uint32_t)__float_as_int(root_lo.w);
-            uint32_t steps = 0;
-            for (;;) {
-                if (pair + 1 >= s.n_fnodes || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); break; }
-                const float4 *p = s.fnodes + 2 * pair;
-                const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-                if (kCount) cnt.nodes += 2;
-                float tl, tr;
-                bool hl = fast_slab(l0, l1, f, best_t, tl);
-                bool hr = fast_slab(r0, r1, f, best_t, tr);
-                const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
-                if (hl && lb > 0) {
-                    fast_leaf<kCount>(s, r, (uint32_t)__float_as_int(l0.w), (uint32_t)lb, best_t, best_i, have, cnt);
-                    hl = false;
-                }
-                if (hr && rb > 0) {
-                    fast_leaf<kCount>(s, r, (uint32_t)__float_as_int(r0.w), (uint32_t)rb, best_t, best_i, have, cnt);
-                    hr = false;
-                }
-                if (hl && hr) {
-                    const bool left_first = tl <= tr;
-                    const uint32_t near_p = (uint32_t)__float_as_int(left_first ? l0.w : r0.w);
-                    const uint32_t far_p = (uint32_t)__float_as_int(left_first ? r0.w : l0.w);
-                    if (sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); break; }
-                    stack_n[sp] = far_p;
-                    stack_t[sp] = left_first ? tr : tl;
-                    ++sp;
-                    pair = near_p;
-                } else if (hl) {
-                    pair = (uint32_t)__float_as_int(l0.w);
-                } else if (hr) {
-                    pair = (uint32_t)__float_as_int(r0.w);
-                } else {
-                    bool found = false;
-                    while (sp > 0) {
-                        --sp;
-                        if (stack_t[sp] <= best_t * 1.000001f) { pair = stack_n[sp]; found = true; break; }
-                    }
-                    if (!found) break;
-                }
+            if (!node_in_range(s, cur) || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); break; }
+            float ct[kWide];
+            uint32_t cc[kWide];
+            const int n = wide_children<true>(s, cur, f, best_t, ct, cc);
+            if (kCount) cnt.nodes += kWide;
+            cur = kNodeNone;
+            if (n > 0) {
+                if (sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); break; }
+#pragma unroll
+                for (int k = kWide - 1; k >= 1; --k)
+                    if (k < n) { stack_n[sp] = cc[k]; stack_t[sp] = ct[k]; ++sp; }
+                cur = cc[0];
             }
         }
     }
@@ -456,56 +517,46 @@ __device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t
     return true;
 }
 
+__device__ __forceinline__ bool fast_occ_leaf(const DevScene &s, const Ray &r, uint32_t first, uint32_t count,
+                                              float dist) {
+    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return false; }
+    for (uint32_t k = first; k < first + count; ++k) {
+        const float4 A = __ldg(&s.ftris[3 * k]);
+        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
+        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+        if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
+        if (tri_occ(v3(A), v3(AB), v3(AC), r, dist)) return true;
+    }
+    return false;
+}
+
 __device__ inline bool fast_occ(const DevScene &s, const Ray &r, float dist) {
     if (s.n_tri == 0) return false;
     const FastRay f = fast_ray(r);
-    const float4 root_lo = __ldg(&s.fnodes[0]), root_hi = __ldg(&s.fnodes[1]);
-    float tn;
-    if (!fast_slab(root_lo, root_hi, f, dist, tn)) return false;
-    const int root_b = __float_as_int(root_hi.w);
-    auto leaf = [&](uint32_t first, uint32_t count) -> bool {
-        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return false; }
-        for (uint32_t k = first; k < first + count; ++k) {
-            const float4 A = __ldg(&s.ftris[3 * k]);
-            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
-            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
-            if (tri_occ(v3(A), v3(AB), v3(AC), r, dist)) return true;
-        }
-        return false;
-    };
-    if (root_b > 0) return leaf((uint32_t)__float_as_int(root_lo.w), (uint32_t)root_b);
     uint32_t stack_n[kFastStack];
     int sp = 0;
-    uint32_t pair = (uint32_t)__float_as_int(root_lo.w);
+    uint32_t cur = 0;
     uint32_t steps = 0;
     for (;;) {
-        if (pair + 1 >= s.n_fnodes || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); return false; }
-        const float4 *p = s.fnodes + 2 * pair;
-        const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-        float tl, tr;
-        bool hl = fast_slab(l0, l1, f, dist, tl);
-        bool hr = fast_slab(r0, r1, f, dist, tr);
-        const int lb = __float_as_int(l1.w), rb = __float_as_int(r1.w);
-        if (hl && lb > 0) {
-            if (leaf((uint32_t)__float_as_int(l0.w), (uint32_t)lb)) return true;
-            hl = false;
-        }
-        if (hr && rb > 0) {
-            if (leaf((uint32_t)__float_as_int(r0.w), (uint32_t)rb)) return true;
-            hr = false;
-        }
-        if (hl && hr) {
-            if (sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); return false; }
-            stack_n[sp++] = (uint32_t)__float_as_int(r0.w);
-            pair = (uint32_t)__float_as_int(l0.w);
-        } else if (hl) {
-            pair = (uint32_t)__float_as_int(l0.w);
-        } else if (hr) {
-            pair = (uint32_t)__float_as_int(r0.w);
-        } else {
+        if (cur == kNodeNone) {
             if (sp == 0) return false;
-            pair = stack_n[--sp];
+            cur = stack_n[--sp];
+        } else if (cur & kLeafCode) {
+            if (fast_occ_leaf(s, r, code_first(cur), code_count(cur), dist)) return true;
+            cur = kNodeNone;
+        } else {
+            if (!node_in_range(s, cur) || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); return false; }
+            float ct[kWide];
+            uint32_t cc[kWide];
+            const int n = wide_children<false>(s, cur, f, dist, ct, cc);
+            cur = kNodeNone;
+            if (n > 0) {
+                if (sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); return false; }
+#pragma unroll
+                for (int k = kWide - 1; k >= 1; --k)
+                    if (k < n) stack_n[sp++] = cc[k];
+                cur = cc[0];
+            }
         }
     }
 }
