@@ -431,6 +431,135 @@ def bench_served(args):
     print(json.dumps(line), flush=True)
 
 
+SCENE_WORKLOADS = {
+    "cornell": ("config 1: Whitted 256x256, 1 spp (Constant 0.5 camera sampler), procedural Cornell box "
+                "(10 wall + 24 box triangles, mirror sphere, 2 area-light triangles of emission 15), BVH"),
+    "terrain": ("config 3: PathTracer 1024x1024, 64 spp HaltonSeq (camera, light and roulette), depth 6 with "
+                "Russian roulette beyond depth 3, 512x512 fBm heightfield (524,288 triangles), 4 area-light quads "
+                "of emission 10, fp32 sums"),
+}
+
+
+def scene_workload(name):
+    from mobileraytracer_b200 import capi, scenes
+    if name == "cornell":
+        sc = scenes.cornell_box()
+        opts = capi.render_opts(shader=capi.MRT_SHADER_WHITTED, width=256, height=256, spp=1, spl=1, seed=1)
+    else:
+        sc = scenes.heightfield(cells=512, seed=1)
+        H = capi.MRT_SAMPLER_HALTON
+        opts = capi.render_opts(shader=capi.MRT_SHADER_PATHTRACER, width=1024, height=1024, spp=64, spl=1,
+                                pixel_sampler=H, light_sampler=H, rr_sampler=H, depth_min=3, depth_max=6, seed=1)
+    return sc, opts
+
+
+def bench_scene(args):
+    """Configs 1 and 3: one step = one Renderer::renderFrame of the frame (mrt_render on device
+    buffers); value = rays traced (camera + secondary + shadow) / device time."""
+    import torch
+    import mobileraytracer_b200 as m
+    from mobileraytracer_b200 import capi
+    sc, opts = scene_workload(args.workload)
+    torch.cuda.set_device(0)
+    ctx = m.Context(0)
+    t0 = time.time()
+    scene = m.Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
+    build_s = time.time() - t0
+    w, h = opts.width, opts.height
+    bitmap = torch.zeros(w * h, dtype=torch.int32, device="cuda")
+    accum = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream, device="cuda")
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)   # evicts L2 (126 MB) before every step; not inside the timed events
+        _, _, st = scene.render(sc.camera, opts, bitmap=bitmap, accum=accum)
+        return st
+
+    clocks = ClockSampler(0).__enter__()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks.mark()
+    dev_ms = 0.0
+    rays = paths = 0
+    for _ in range(args.steps):
+        st = step()
+        dev_ms += st.device_ms
+        rays += st.rays_closest + st.rays_shadow
+        paths += st.paths
+    torch.cuda.synchronize()
+    clocks.__exit__(None, None, None)
+    value = rays / (dev_ms / 1e3) / 1e6
+    rays_per_path = rays / paths
+    # end to end: host bitmap and sums in and out through the C ABI
+    host_bm = np.zeros((h, w), np.uint32)
+    host_acc = np.zeros((h, w, 4), np.float32)
+    scene.render(sc.camera, opts, bitmap=host_bm, accum=host_acc)
+    n_e2e = max(1, min(args.e2e_steps, args.steps))
+    t1 = time.perf_counter()
+    for _ in range(n_e2e):
+        scene.render(sc.camera, opts, bitmap=host_bm, accum=host_acc)
+    e2e_s = (time.perf_counter() - t1) / n_e2e
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = scene_cpu_baseline(sc, opts, rays_per_path, args.cpu_budget)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": SCENE_WORKLOADS[args.workload], "rays_per_step": rays / args.steps,
+                   "paths_per_step": paths / args.steps, "rays_per_path": rays_per_path,
+                   "samples_per_s": paths / (dev_ms / 1e3), "bvh_build_seconds": build_s,
+                   "l2": "flushed before every step (512 MiB write outside the timed events)"},
+        "e2e": {"value": rays / args.steps / e2e_s / 1e6, "unit": "Mrays/s",
+                "h2d_bytes_per_step": host_bm.nbytes + host_acc.nbytes,
+                "d2h_bytes_per_step": host_bm.nbytes + host_acc.nbytes},
+        "gpu_launches": None, "roofline": None, "clocks": clocks.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+
+
+def scene_cpu_baseline(sc, opts, rays_per_path: float, budget_s: float):
+    """The reference's CPU renderer (oracle/_ref, its release optimisation level) on the host cores.
+    It traces but does not count rays, so its Mrays/s is its camera paths per second times the rays
+    per path the device counted on the same frame."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc as O
+    from mobileraytracer_b200 import capi
+    threads = os.cpu_count() or 1
+    try:
+        O.ref(fast=True)
+    except Exception as e:  # the checker library was not built
+        log(f"cpu baseline unavailable: {e}")
+        return None
+    if opts.width * opts.height * opts.spp <= 1 << 17:   # small frame: whole frames, repeated
+        n, t = 0, 0.0
+        while t < budget_s / 4:
+            _, _, tr = O.ref_render(sc, sc.camera, opts, capi.MRT_ACCEL_BVH, threads, fast=True)
+            n += 1
+            t += tr
+        paths = n * opts.width * 16 * (opts.height // 16) * opts.spp
+        sample = f"{n} whole {opts.width}x{opts.height} frames, reference BVH, {threads} threads"
+    else:                                                # one sample of every step-th pixel
+        total = opts.width * opts.height
+        one = capi.render_opts(shader=opts.shader, width=opts.width, height=opts.height, spp=1, spl=opts.spl,
+                               pixel_sampler=opts.pixel_sampler, light_sampler=opts.light_sampler,
+                               rr_sampler=opts.rr_sampler, depth_min=opts.depth_min, depth_max=opts.depth_max,
+                               seed=opts.seed)
+        _, n0, _, tr0 = O.ref_render_subset(sc, sc.camera, one, capi.MRT_ACCEL_BVH, threads, 0,
+                                            max(1, total // (threads * 16)))
+        step = max(1, int(total / max(1.0, n0 / max(tr0, 1e-6) * budget_s)))
+        _, paths, _, t = O.ref_render_subset(sc, sc.camera, one, capi.MRT_ACCEL_BVH, threads, 1, step)
+        sample = (f"sample 0 of every {step}th pixel of the {opts.width}x{opts.height} frame ({paths} camera paths), "
+                  f"reference BVH and samplers, {threads} threads")
+    return {"value": paths * rays_per_path / t / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": sample, "paths_per_s": paths / t, "rays_per_path_assumed": rays_per_path}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -440,9 +569,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="frame", choices=["frame", "batched", "served"],
-                    help="frame: the 1920x1080 NoShadows frame (default); batched: the 256-job batch; "
-                         "served: the request stream")
+    ap.add_argument("--workload", default="frame", choices=["frame", "cornell", "terrain", "batched", "served"],
+                    help="frame: the 1920x1080 NoShadows frame (default); cornell / terrain: the Whitted and "
+                         "PathTracer frames; batched: the 256-job batch; served: the request stream")
     ap.add_argument("--duration", type=float, default=120.0, help="served: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=50.0, help="served: arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: device footprint budget")
@@ -453,7 +582,7 @@ def main():
                     help="batched: which jobs fill a wave")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 1 if args.workload == "batched" else 200
+        args.steps = {"batched": 1, "terrain": 3}.get(args.workload, 200)
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
@@ -463,6 +592,9 @@ def main():
         return
     if args.workload == "served":
         bench_served(args)
+        return
+    if args.workload in SCENE_WORKLOADS:
+        bench_scene(args)
         return
 
     import torch
