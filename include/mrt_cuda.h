@@ -63,10 +63,15 @@ extern "C" {
 #define MRT_GRID_INDEX_REFERENCE 0
 #define MRT_GRID_INDEX_LINEAR 1
 
-/* c_wrapper.cpp:444-486 shader codes: 1 Whitted, 2 PathTracer, default NoShadows */
+/* c_wrapper.cpp:444-486 shader codes: 1 Whitted, 2 PathTracer, 3 DepthMap, 4 DiffuseMaterial,
+ * default NoShadows.  DEPTHMAP (DepthMap.cpp:19-26) shades a hit grey by its distance against
+ * MrtRenderOpts.depth_point; DIFFUSE (DiffuseMaterial.cpp:16-38) by the first non-zero of the
+ * material's Kd, Ks, Kt, Le (the primitive colour without material). */
 #define MRT_SHADER_NOSHADOWS 0
 #define MRT_SHADER_WHITTED 1
 #define MRT_SHADER_PATHTRACER 2
+#define MRT_SHADER_DEPTHMAP 3
+#define MRT_SHADER_DIFFUSE 4
 
 /* Samplers (app/Components/Samplers).  The reference draws from std::mt19937 seeded from
  * /dev/urandom and from process-wide atomic counters, so it is not reproducible; here every draw is
@@ -85,7 +90,8 @@ extern "C" {
 #define MRT_LIGHT_POINT 0 /* Components::PointLight (PointLight.cpp:17-26) */
 #define MRT_LIGHT_AREA 1  /* Components::AreaLight  (AreaLight.cpp:22-43)  */
 
-#define MRT_CAMERA_PERSPECTIVE 0 /* Components::Perspective (Perspective.cpp:24-44) */
+#define MRT_CAMERA_PERSPECTIVE 0  /* Components::Perspective (Perspective.cpp:24-44) */
+#define MRT_CAMERA_ORTHOGRAPHIC 1 /* Components::Orthographic (Orthographic.cpp:23-46) */
 
 /* Hit ids: primitive type in the top two bits, index inside that type's array below. */
 #define MRT_PRIM_PLANE 0u
@@ -144,7 +150,10 @@ typedef struct MrtAccelOpts {
     int32_t bvh_mode;          /* MRT_BVH_* */
     int32_t grid_size;         /* 0 = the reference rule (Shader.cpp:76-105); > 0 forces G for triangles */
     int32_t grid_index;        /* MRT_GRID_INDEX_* */
-    float camera_position[3];  /* grid bounds include the camera (Shader.cpp:56-62) */
+    float camera_position[3];  /* grid bounds include the camera (Shader.cpp:56-62) ... */
+    const struct MrtCamera *camera;   /* ... or, when not NULL, this camera's getAABB (a point for
+                                         Perspective, the film rectangle for Orthographic,
+                                         Camera.cpp:39-44, Orthographic.cpp:36-46) */
 } MrtAccelOpts;
 
 /* MobileRT::Ray (app/MobileRT/Ray.hpp:14-17); exclude = hit id of the primitive the ray leaves
@@ -162,12 +171,12 @@ typedef struct MrtHit {
 } MrtHit;
 
 typedef struct MrtCamera {
-    int32_t kind;         /* MRT_CAMERA_PERSPECTIVE */
+    int32_t kind;         /* MRT_CAMERA_PERSPECTIVE or MRT_CAMERA_ORTHOGRAPHIC */
     float position[3];
     float look_at[3];
     float up[3];
-    float fov_h_deg;      /* Perspective(position, lookAt, up, hFov, vFov), degrees */
-    float fov_v_deg;
+    float fov_h_deg;      /* Perspective(position, lookAt, up, hFov, vFov): degrees;       */
+    float fov_v_deg;      /* Orthographic(position, lookAt, up, sizeH, sizeV): film size    */
 } MrtCamera;
 
 typedef struct MrtRenderOpts {
@@ -186,6 +195,8 @@ typedef struct MrtRenderOpts {
     uint32_t spp_offset;    /* index of the first sample: a progressive render continues the stream
                                and the running mean from here */
     uint32_t reserved;
+    float depth_point[3];   /* DepthMap maxPoint (DepthMap.cpp:14-17): depth = max(1 - t / (2 |p - o|), 0) */
+    uint32_t reserved2;
 } MrtRenderOpts;
 
 typedef struct MrtRenderStats {

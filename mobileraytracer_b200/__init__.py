@@ -115,12 +115,19 @@ class Scene:
         ctx._scenes.add(self)
 
     def build(self, accelerator: int = capi.MRT_ACCEL_BVH, bvh_mode: int = capi.MRT_BVH_FAST, grid_size: int = 0,
-              grid_index: int = capi.MRT_GRID_INDEX_REFERENCE, camera_position=None):
+              grid_index: int = capi.MRT_GRID_INDEX_REFERENCE, camera_position=None, camera=None):
+        """Shader::initializeAccelerators.  Grid bounds include `camera` (its getAABB), else the point
+        `camera_position`, else the scene's own camera."""
         o = capi.MrtAccelOpts()
         o.accelerator, o.bvh_mode, o.grid_size, o.grid_index = accelerator, bvh_mode, grid_size, grid_index
+        if camera is None and camera_position is None and self.host.camera is not None:
+            camera = self.host.camera
         if camera_position is None:
-            camera_position = list(self.host.camera.position) if self.host.camera is not None else [0.0, 0.0, 0.0]
+            camera_position = list(camera.position) if camera is not None else [0.0, 0.0, 0.0]
         o.camera_position[:] = camera_position
+        if camera is not None:
+            self._build_camera = camera
+            o.camera = ctypes.pointer(camera)
         self.ctx.check(self.lib.mrt_scene_build(self.h, ctypes.byref(o)), "mrt_scene_build")
         return self
 

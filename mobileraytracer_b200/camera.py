@@ -5,7 +5,8 @@ generate (e.g. for the counting replay behind the roofline figure).  numpy float
 IEEE binary32 with no fused multiply-add, so with the reference's operation order the rays equal the
 device ones bit for bit (checked against the oracle in tests/test_camera.py):
   Camera ctor (Camera.cpp:52-57), Perspective ctor and generateRay / fastArcTan
-  (Perspective.cpp:10-44), pixel loop u = x / W, v = y / H (Renderer.cpp:94-104).
+  (Perspective.cpp:10-44), Orthographic ctor and generateRay (Orthographic.cpp:12-34), pixel loop
+  u = x / W, v = y / H (Renderer.cpp:94-104).
 """
 from __future__ import annotations
 
@@ -63,13 +64,20 @@ def primary_rays(cam: capi.MrtCamera, width: int, height: int, pixels: np.ndarra
     du = (j - F(0.5)) * F(2.0) * pw
     dv = (j - F(0.5)) * F(2.0) * ph
     pos, direction, right, up, hfov, vfov = basis(cam)
+    r = np.zeros(len(pixels), RAY_DTYPE)
+    r["depth"] = 1
+    r["exclude"] = 0xFFFFFFFF
+    if cam.kind == capi.MRT_CAMERA_ORTHOGRAPHIC:   # Orthographic.cpp:12-34
+        sh, sv = F(cam.fov_h_deg) / F(2.0), F(cam.fov_v_deg) / F(2.0)
+        rgt = right[None, :] * ((u - F(0.5)) * sh)[:, None] + right[None, :] * du
+        upv = up[None, :] * ((F(0.5) - v) * sv)[:, None] + up[None, :] * dv
+        r["origin"] = ((pos[None, :] + rgt) + upv).astype(F)
+        r["direction"] = direction
+        return r
     rf = _fast_arctan(hfov * (u - F(0.5))) + du
     uf = _fast_arctan(vfov * (F(0.5) - v)) + dv
     dest = ((pos + direction)[None, :] + right[None, :] * rf[:, None]) + up[None, :] * uf[:, None]
     d = _normalize(dest - pos[None, :])
-    r = np.zeros(len(pixels), RAY_DTYPE)
     r["origin"] = pos
     r["direction"] = d.astype(F)
-    r["depth"] = 1
-    r["exclude"] = 0xFFFFFFFF
     return r

@@ -16,10 +16,10 @@ MRT_OK, MRT_ERR_ARG, MRT_ERR_OOM, MRT_ERR_CUDA, MRT_ERR_LIMIT, MRT_ERR_CANCELLED
 MRT_ACCEL_NAIVE, MRT_ACCEL_REGULAR_GRID, MRT_ACCEL_BVH = 0, 1, 2
 MRT_BVH_FAST, MRT_BVH_REFERENCE = 0, 1
 MRT_GRID_INDEX_REFERENCE, MRT_GRID_INDEX_LINEAR = 0, 1
-MRT_SHADER_NOSHADOWS, MRT_SHADER_WHITTED, MRT_SHADER_PATHTRACER = 0, 1, 2
+MRT_SHADER_NOSHADOWS, MRT_SHADER_WHITTED, MRT_SHADER_PATHTRACER, MRT_SHADER_DEPTHMAP, MRT_SHADER_DIFFUSE = 0, 1, 2, 3, 4
 MRT_SAMPLER_CONSTANT, MRT_SAMPLER_STRATIFIED, MRT_SAMPLER_HALTON, MRT_SAMPLER_RANDOM = 0, 1, 2, 3
 MRT_LIGHT_POINT, MRT_LIGHT_AREA = 0, 1
-MRT_CAMERA_PERSPECTIVE = 0
+MRT_CAMERA_PERSPECTIVE, MRT_CAMERA_ORTHOGRAPHIC = 0, 1
 MRT_PRIM_PLANE, MRT_PRIM_SPHERE, MRT_PRIM_TRIANGLE, MRT_PRIM_LIGHT = 0, 1, 2, 3
 MRT_HIT_NONE = 0xFFFFFFFF
 MRT_MEM_HOST, MRT_MEM_DEVICE = 0, 1
@@ -64,9 +64,15 @@ class MrtSceneDesc(ctypes.Structure):
     ]
 
 
+class MrtCamera(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("position", ctypes.c_float * 3), ("look_at", ctypes.c_float * 3),
+                ("up", ctypes.c_float * 3), ("fov_h_deg", ctypes.c_float), ("fov_v_deg", ctypes.c_float)]
+
+
 class MrtAccelOpts(ctypes.Structure):
     _fields_ = [("accelerator", ctypes.c_int32), ("bvh_mode", ctypes.c_int32), ("grid_size", ctypes.c_int32),
-                ("grid_index", ctypes.c_int32), ("camera_position", ctypes.c_float * 3)]
+                ("grid_index", ctypes.c_int32), ("camera_position", ctypes.c_float * 3),
+                ("camera", ctypes.POINTER(MrtCamera))]
 
 
 class MrtRay(ctypes.Structure):
@@ -78,18 +84,14 @@ class MrtHit(ctypes.Structure):
     _fields_ = [("t", ctypes.c_float), ("id", ctypes.c_uint32)]
 
 
-class MrtCamera(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("position", ctypes.c_float * 3), ("look_at", ctypes.c_float * 3),
-                ("up", ctypes.c_float * 3), ("fov_h_deg", ctypes.c_float), ("fov_v_deg", ctypes.c_float)]
-
-
 class MrtRenderOpts(ctypes.Structure):
     _fields_ = [
         ("shader", ctypes.c_int32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
         ("spp", ctypes.c_uint32), ("spl", ctypes.c_uint32), ("pixel_sampler", ctypes.c_int32),
         ("constant_value", ctypes.c_float), ("light_sampler", ctypes.c_int32), ("rr_sampler", ctypes.c_int32),
         ("depth_min", ctypes.c_int32), ("depth_max", ctypes.c_int32), ("seed", ctypes.c_uint64),
-        ("spp_offset", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("spp_offset", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("depth_point", ctypes.c_float * 3),
+        ("reserved2", ctypes.c_uint32),
     ]
 
 
@@ -120,7 +122,7 @@ class MrtBatchStats(ctypes.Structure):
 
 def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1, pixel_sampler=None,
                 constant_value=0.5, light_sampler=MRT_SAMPLER_RANDOM, rr_sampler=MRT_SAMPLER_RANDOM,
-                depth_min=4, depth_max=8, seed=0, spp_offset=0) -> MrtRenderOpts:
+                depth_min=4, depth_max=8, seed=0, spp_offset=0, depth_point=(1.0, 1.0, 1.0)) -> MrtRenderOpts:
     """Options with the reference CLI's wiring as defaults (c_wrapper.cpp:436-443,455): the pixel
     sampler is Constant(0.5) at 1 spp and random otherwise; RayDepthMin 4, RayDepthMax 8."""
     if pixel_sampler is None:
@@ -130,6 +132,7 @@ def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1
     o.pixel_sampler, o.constant_value = pixel_sampler, constant_value
     o.light_sampler, o.rr_sampler = light_sampler, rr_sampler
     o.depth_min, o.depth_max, o.seed, o.spp_offset = depth_min, depth_max, seed, spp_offset
+    o.depth_point[:] = depth_point
     return o
 
 

@@ -183,9 +183,11 @@ public:
     void initializeAccelerators(Camera *camera) noexcept;
     virtual void resetSampling() noexcept {}
 
-    // which shade() the GPU runs (c_wrapper.cpp:444-486 codes: 0 NoShadows, 1 Whitted, 2 PathTracer)
+    // which shade() the GPU runs (c_wrapper.cpp:444-486 codes: 0 NoShadows, 1 Whitted, 2 PathTracer,
+    // 3 DepthMap, 4 DiffuseMaterial)
     virtual int shaderKind() const noexcept = 0;
     virtual const Sampler *russianRoulette() const noexcept { return nullptr; }
+    virtual detail::F3 depthPoint() const noexcept { return detail::F3{}; }
     std::uint32_t samplesLight() const noexcept { return samplesLight_; }
     Accelerator accelerator() const noexcept { return accelerator_; }
 
@@ -259,6 +261,22 @@ private:
     float hFov_{}, vFov_{};
 };
 
+// Orthographic.hpp:12-45
+class Orthographic final : public ::MobileRT::Camera {
+public:
+    explicit Orthographic(const ::glm::vec3 &position, const ::glm::vec3 &lookAt, const ::glm::vec3 &up, float sizeH,
+                          float sizeV) noexcept
+        : Camera{position, lookAt, up}, sizeH_{sizeH}, sizeV_{sizeV} {}
+    int kind() const noexcept final { return 1; }
+    float hFovDegrees() const noexcept final { return sizeH_; }   // the film size, for the C ABI
+    float vFovDegrees() const noexcept final { return sizeV_; }
+    float getSizeH() const noexcept { return sizeH_ / 2.0f; }     // the reference keeps half the size
+    float getSizeV() const noexcept { return sizeV_ / 2.0f; }
+
+private:
+    float sizeH_{}, sizeV_{};
+};
+
 // Constant.hpp, Stratified.hpp, HaltonSeq.hpp, MersenneTwister.hpp
 class Constant final : public ::MobileRT::Sampler {
 public:
@@ -321,6 +339,24 @@ public:
 
 private:
     std::unique_ptr<::MobileRT::Sampler> samplerRussianRoulette_{};
+};
+
+// DepthMap.hpp, DiffuseMaterial.hpp
+class DepthMap final : public ::MobileRT::Shader {
+public:
+    explicit DepthMap(::MobileRT::Scene &&scene, const ::glm::vec3 &maxPoint, Accelerator accelerator) noexcept
+        : Shader{std::move(scene), 0, accelerator}, maxPoint_{::MobileRT::detail::f3(maxPoint)} {}
+    int shaderKind() const noexcept final { return 3; }
+    ::MobileRT::detail::F3 depthPoint() const noexcept final { return maxPoint_; }
+
+private:
+    ::MobileRT::detail::F3 maxPoint_{};
+};
+class DiffuseMaterial final : public ::MobileRT::Shader {
+public:
+    explicit DiffuseMaterial(::MobileRT::Scene &&scene, Accelerator accelerator) noexcept
+        : Shader{std::move(scene), 0, accelerator} {}
+    int shaderKind() const noexcept final { return 4; }
 };
 
 }  // namespace Components

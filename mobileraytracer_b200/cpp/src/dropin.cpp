@@ -29,6 +29,15 @@ MrtContext *context() {
     return ctx;
 }
 
+MrtCamera to_mrt(const Camera &camera) {
+    MrtCamera c{};
+    c.kind = camera.kind();
+    for (int k = 0; k < 3; ++k) { c.position[k] = camera.position_.v[k]; c.look_at[k] = camera.lookAt_.v[k]; c.up[k] = camera.up_.v[k]; }
+    c.fov_h_deg = camera.hFovDegrees();
+    c.fov_v_deg = camera.vFovDegrees();
+    return c;
+}
+
 std::string context_error(MrtContext *ctx, int st, const char *what) {
     return std::string(what) + ": status " + std::to_string(st) + ": " + (ctx ? mrt_context_error(ctx) : "no CUDA context");
 }
@@ -137,7 +146,12 @@ void Shader::initializeAccelerators(Camera *camera) noexcept {
     o.bvh_mode = bvhMode_;
     o.grid_size = gridSize_;
     o.grid_index = gridIndex_;
-    if (camera) { o.camera_position[0] = camera->position_.v[0]; o.camera_position[1] = camera->position_.v[1]; o.camera_position[2] = camera->position_.v[2]; }
+    MrtCamera cam{};
+    if (camera) {
+        o.camera_position[0] = camera->position_.v[0]; o.camera_position[1] = camera->position_.v[1]; o.camera_position[2] = camera->position_.v[2];
+        cam = to_mrt(*camera);
+        o.camera = &cam;   // grid bounds take the camera's getAABB (Shader.cpp:56-62)
+    }
     st = mrt_scene_build(s, &o);
     if (st != MRT_OK) {
         error_ = context_error(ctx, st, "mrt_scene_build");
@@ -176,11 +190,9 @@ void Renderer::renderFrame(std::uint32_t *bitmap, std::int32_t /*numThreads*/, s
     o.depth_min = depthMin_;
     o.depth_max = depthMax_;
     o.seed = seed_;
-    MrtCamera c{};
-    c.kind = camera_->kind();
-    for (int k = 0; k < 3; ++k) { c.position[k] = camera_->position_.v[k]; c.look_at[k] = camera_->lookAt_.v[k]; c.up[k] = camera_->up_.v[k]; }
-    c.fov_h_deg = camera_->hFovDegrees();
-    c.fov_v_deg = camera_->vFovDegrees();
+    const detail::F3 dp = shader_->depthPoint();
+    for (int k = 0; k < 3; ++k) o.depth_point[k] = dp.v[k];
+    const MrtCamera c = to_mrt(*camera_);
     const int st = mrt_render(shader_->device_->scene, &c, &o, bitmap, stride, nullptr, MRT_MEM_HOST, nullptr);
     if (st != MRT_OK && st != MRT_ERR_CANCELLED) {
         error_ = context_error(context(), st, "mrt_render");

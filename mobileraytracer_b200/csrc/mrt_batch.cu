@@ -204,8 +204,9 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_shadow(BatchSta
     }
 }
 
-// NoShadows::shade (NoShadows.cpp:19-65) in node form: the value is final at the camera ray
-__device__ __forceinline__ void shade_noshadows_node(const DevScene &s, const RenderParams &p, const RayRec &rr,
+// NoShadows / DepthMap / DiffuseMaterial (NoShadows.cpp:19-65, DepthMap.cpp:19-26,
+// DiffuseMaterial.cpp:16-38) in node form: the value is final at the camera ray
+__device__ __forceinline__ void shade_direct_node(const DevScene &s, const RenderParams &p, const RayRec &rr,
                                                      uint32_t hit_id, float hit_t, const Stream &st, ShadeLane &o) {
     o.n_child = 0;
     o.n_shadow = 0;
@@ -224,7 +225,7 @@ __device__ __forceinline__ void shade_noshadows_node(const DevScene &s, const Re
     Isect it;
     if (!make_isect(s, r, hit_id, it)) return;
     nd.flags = kEmit;   // resolves to the value in `point`
-    nd.point = shade_noshadows(s, p, st, it, 1u);
+    nd.point = shade_direct(s, p, st, r, it);
 }
 
 __global__ void __launch_bounds__(128) k_batch_shade(BatchState b, int level) {
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(128) k_batch_shade(BatchState b, int level) {
             const DevScene &s = b.scenes[job];
             st = stream_of(p, b.root_local[rr.root]);
             const NodeRec &in = b.nodes[idx];
-            if (p.shader == MRT_SHADER_NOSHADOWS) shade_noshadows_node(s, p, rr, in.hit_id, in.hit_t, st, o);
+            if (direct_shader(p.shader)) shade_direct_node(s, p, rr, in.hit_id, in.hit_t, st, o);
             else shade_ray(s, p, rr, in.hit_id, in.hit_t, st, o);
             b.nodes[idx] = o.nd;
         }
@@ -798,8 +799,9 @@ int mrt_batch_submit(MrtBatch *b, const MrtBatchJob *job, uint64_t *job_id) {
         set_error(ctx, "mrt_batch_submit: the scene must be built with MRT_ACCEL_BVH + MRT_BVH_FAST on the batch's device");
         return MRT_ERR_ARG;
     }
-    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_PATHTRACER || o->spp == 0 || o->spl == 0 ||
-        job->camera.kind != MRT_CAMERA_PERSPECTIVE || o->pixel_sampler < 0 || o->pixel_sampler > 3 ||
+    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_DIFFUSE || o->spp == 0 ||
+        (o->spl == 0 && (o->shader == MRT_SHADER_WHITTED || o->shader == MRT_SHADER_PATHTRACER || o->shader == MRT_SHADER_NOSHADOWS)) ||
+        (job->camera.kind != MRT_CAMERA_PERSPECTIVE && job->camera.kind != MRT_CAMERA_ORTHOGRAPHIC) || o->pixel_sampler < 0 || o->pixel_sampler > 3 ||
         o->light_sampler < 0 || o->light_sampler > 3 || o->rr_sampler < 0 || o->rr_sampler > 3 || !job->bitmap) {
         set_error(ctx, "mrt_batch_submit: invalid options");
         return MRT_ERR_ARG;
@@ -809,7 +811,7 @@ int mrt_batch_submit(MrtBatch *b, const MrtBatchJob *job, uint64_t *job_id) {
                        "height / (height / 16) == 16");
         return MRT_ERR_ARG;
     }
-    if (o->depth_max > (int)b->opts.max_depth || o->spl > b->opts.max_spl) {
+    if (!direct_shader(o->shader) && (o->depth_max > (int)b->opts.max_depth || o->spl > b->opts.max_spl)) {
         set_error(ctx, "mrt_batch_submit: depth_max above the batch's max_depth (%u) or samplesLight above max_spl (%u)",
                   b->opts.max_depth, b->opts.max_spl);
         return MRT_ERR_ARG;
@@ -844,6 +846,7 @@ int mrt_batch_submit(MrtBatch *b, const MrtBatchJob *job, uint64_t *job_id) {
     p.inv_h = 1.0f / (float)o->height;
     p.pw = 0.5f / (float)o->width;
     p.ph = 0.5f / (float)o->height;
+    p.depth_point = V3{o->depth_point[0], o->depth_point[1], o->depth_point[2]};
     b->h_jobs[slot] = p;
     b->h_scenes[slot] = s->dev;
     b->h_scenes[slot].error_flag = ctx->d_error;

@@ -144,10 +144,31 @@ DevCamera make_camera(const MrtCamera &c) {
     k.direction = h_normalize(V3{c.look_at[0], c.look_at[1], c.look_at[2]} - k.position);
     k.right = cross(V3{c.up[0], c.up[1], c.up[2]}, k.direction);
     k.up = cross(k.direction, k.right);
+    k.kind = c.kind;
+    if (c.kind == MRT_CAMERA_ORTHOGRAPHIC) {   // Orthographic.cpp:12-17: half the film size
+        k.hfov = c.fov_h_deg / 2.0f;
+        k.vfov = c.fov_v_deg / 2.0f;
+        return k;
+    }
     const float pi = 3.14159265358979323846f;
     k.hfov = (c.fov_h_deg * pi) / 180.0f;
     k.vfov = (c.fov_v_deg * pi) / 180.0f;
     return k;
+}
+
+// Camera::getAABB (Camera.cpp:39-44: the position) and Orthographic::getAABB (Orthographic.cpp:36-46:
+// two corners of the film rectangle, in the reference's order of operations)
+void camera_box(const MrtCamera &c, float *mn, float *mx) {
+    const DevCamera k = make_camera(c);
+    V3 a = k.position, b = k.position;
+    if (c.kind == MRT_CAMERA_ORTHOGRAPHIC) {
+        a = (((k.position + (k.right * (0.0f - 0.5f)) * k.hfov) + k.right * -0.5f) + (k.up * (0.5f - 0.0f)) * k.vfov) +
+            k.up * -0.5f;
+        b = (((k.position + (k.right * (1.0f - 0.5f)) * k.hfov) + k.right * 0.5f) + (k.up * (0.5f - 1.0f)) * k.vfov) +
+            k.up * 0.5f;
+    }
+    mn[0] = a.x; mn[1] = a.y; mn[2] = a.z;
+    mx[0] = b.x; mx[1] = b.y; mx[2] = b.z;
 }
 
 }  // namespace mrt_host
@@ -458,7 +479,12 @@ int mrt_scene_build(MrtScene *s, const MrtAccelOpts *o) {
     s->dev.bvh_mode = o->bvh_mode;
     int st = MRT_OK;
     if (o->accelerator == MRT_ACCEL_BVH) st = o->bvh_mode == MRT_BVH_FAST ? build_fast_bvh(s) : build_reference_bvh(s);
-    else if (o->accelerator == MRT_ACCEL_REGULAR_GRID) st = build_grids(s, o->camera_position, o->grid_size, o->grid_index);
+    else if (o->accelerator == MRT_ACCEL_REGULAR_GRID) {
+        float cmn[3] = {o->camera_position[0], o->camera_position[1], o->camera_position[2]};
+        float cmx[3] = {cmn[0], cmn[1], cmn[2]};
+        if (o->camera) camera_box(*o->camera, cmn, cmx);
+        st = build_grids(s, cmn, cmx, o->grid_size, o->grid_index);
+    }
     if (st != MRT_OK) return st;
     st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "mrt_scene_build");
     if (st == MRT_OK) s->built = true;

@@ -364,7 +364,8 @@ MRT_HD V3 hemisphere(V3 n, float u1, float u2) {
 // ---------------------------------------------------------------------------------------------
 struct DevCamera {
     V3 position, direction, right, up;
-    float hfov, vfov;
+    float hfov, vfov;   // Perspective: field of view in radians; Orthographic: half film size
+    int32_t kind;       // MRT_CAMERA_*
 };
 
 MRT_HD float fast_arctan(float x) {
@@ -373,6 +374,18 @@ MRT_HD float fast_arctan(float x) {
 }
 
 MRT_HD Ray camera_ray(const DevCamera &k, float u, float v, float du, float dv) {
+    if (k.kind == MRT_CAMERA_ORTHOGRAPHIC) {   // Orthographic::generateRay, Orthographic.cpp:23-34
+        const float rf = (u - 0.5f) * k.hfov;
+        const V3 right = k.right * rf + k.right * du;
+        const float uf = (0.5f - v) * k.vfov;
+        const V3 up = k.up * uf + k.up * dv;
+        Ray r;
+        r.d = k.direction;
+        r.o = (k.position + right) + up;
+        r.depth = 1;
+        r.exclude = MRT_HIT_NONE;
+        return r;
+    }
     const float rf = fast_arctan(k.hfov * (u - 0.5f)) + du;
     const V3 right = k.right * rf;
     const float uf = fast_arctan(k.vfov * (0.5f - v)) + dv;

@@ -241,7 +241,7 @@ void launch_fill(MrtScene *s, const GridBuildParams &p, uint32_t n, uint32_t *co
 
 namespace mrt_host {
 
-int build_grids(MrtScene *s, const float *cam, int grid_size, int grid_index) {
+int build_grids(MrtScene *s, const float *cam_min, const float *cam_max, int grid_size, int grid_index) {
     MrtContext *ctx = s->ctx;
     cudaStream_t q = ctx->stream;
     for (int type = 0; type < 3; ++type) {
@@ -253,9 +253,8 @@ int build_grids(MrtScene *s, const float *cam, int grid_size, int grid_index) {
             mn = vmin(b.mn, mn);
             mx = vmax(b.mx, mx);
         }
-        const V3 c{cam[0], cam[1], cam[2]};
-        mn = vmin(c, mn);
-        mx = vmax(c, mx);
+        mn = vmin(V3{cam_min[0], cam_min[1], cam_min[2]}, mn);
+        mx = vmax(V3{cam_max[0], cam_max[1], cam_max[2]}, mx);
         const V3 bmn = subs(mn, kEpsilon), bmx = adds(mx, kEpsilon);
         int32_t G = grid_size_rule(n);
         if (type == kTriangle && grid_size > 0) G = grid_size;

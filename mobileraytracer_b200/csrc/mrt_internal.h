@@ -97,7 +97,7 @@ int check_kernel_error(MrtContext *ctx);                // reads and clears the 
 // builds (mrt_bvh.cu, mrt_grid.cu)
 int build_fast_bvh(MrtScene *s);
 int build_reference_bvh(MrtScene *s);
-int build_grids(MrtScene *s, const float *camera_position, int grid_size, int grid_index);
+int build_grids(MrtScene *s, const float *camera_min, const float *camera_max, int grid_size, int grid_index);
 
 // kernels (mrt_kernels.cu)
 int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits);
@@ -107,5 +107,6 @@ int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *
            float *d_accum, MrtRenderStats *stats);
 
 mrt::DevCamera make_camera(const MrtCamera &c);
+void camera_box(const MrtCamera &c, float *mn, float *mx);
 
 }  // namespace mrt_host

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
             uint32_t id;
             if (scene_closest<ACCEL, MODE>(s, r, len, id)) {
                 Isect it;
-                if (make_isect(s, r, id, it)) rgb = shade_noshadows(s, p, st, it, 1u);
+                if (make_isect(s, r, id, it)) rgb = shade_direct(s, p, st, r, it);
             }
             bm = incremental_avg(rgb, bm, sample + 1u);
             acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
@@ -110,7 +110,7 @@ struct NsWork {
             Isect it;
             if (make_isect(*s, r, id, it)) {
                 const Stream st = make_stream(p->seed, lane.pixel, sample, p->strata, p->constant_value);
-                rgb = shade_noshadows(*s, *p, st, it, 1u);
+                rgb = shade_direct(*s, *p, st, r, it);
             }
         }
         lane.bm = incremental_avg(rgb, lane.bm, sample + 1u);
@@ -486,6 +486,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     p.inv_h = 1.0f / (float)o->height;
     p.pw = 0.5f / (float)o->width;
     p.ph = 0.5f / (float)o->height;
+    p.depth_point = V3{o->depth_point[0], o->depth_point[1], o->depth_point[2]};
     p.n_tasks = plan.n_tasks;
     int st = MRT_OK;
     if (!plan.implicit) {
@@ -522,7 +523,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     uint64_t rays_closest = 0, rays_shadow = 0;
     s->progress.store(0);
     cudaEventRecord(ctx->ev0, q);
-    if (o->shader == MRT_SHADER_NOSHADOWS) {
+    if (direct_shader(o->shader)) {
         const bool fast = accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST;
         const uint32_t rows = 16u * (o->height / 16u);
         const uint32_t tiles_x = (plan.implicit && o->width % 8u == 0 && rows % 4u == 0) ? o->width / 8u : 0u;
@@ -617,8 +618,9 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
     if (!s || !cam || !o || !bitmap) return MRT_ERR_ARG;
     MrtContext *ctx = s->ctx;
     if (!s->built) { set_error(ctx, "mrt_render before mrt_scene_build"); return MRT_ERR_STATE; }
-    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_PATHTRACER || o->spp == 0 || o->spl == 0 ||
-        o->width < 16 || o->height < 16 || stride_bytes < 4u * o->width || cam->kind != MRT_CAMERA_PERSPECTIVE ||
+    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_DIFFUSE || o->spp == 0 ||
+        (o->spl == 0 && (o->shader == MRT_SHADER_WHITTED || o->shader == MRT_SHADER_PATHTRACER || o->shader == MRT_SHADER_NOSHADOWS)) ||
+        o->width < 16 || o->height < 16 || stride_bytes < 4u * o->width || (cam->kind != MRT_CAMERA_PERSPECTIVE && cam->kind != MRT_CAMERA_ORTHOGRAPHIC) ||
         o->pixel_sampler < 0 || o->pixel_sampler > 3 || o->light_sampler < 0 || o->light_sampler > 3 ||
         o->rr_sampler < 0 || o->rr_sampler > 3) {
         set_error(ctx, "mrt_render: invalid options");
@@ -728,8 +730,9 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
     if (!s || !cam || !o || !bitmap) return MRT_ERR_ARG;
     MrtContext *ctx = s->ctx;
     if (!s->built) { set_error(ctx, "mrt_render_noalloc before mrt_scene_build"); return MRT_ERR_STATE; }
-    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_PATHTRACER || o->spp == 0 || o->spl == 0 ||
-        o->width < 16 || o->height < 16 || cam->kind != MRT_CAMERA_PERSPECTIVE || o->pixel_sampler < 0 ||
+    if (o->shader < MRT_SHADER_NOSHADOWS || o->shader > MRT_SHADER_DIFFUSE || o->spp == 0 ||
+        (o->spl == 0 && (o->shader == MRT_SHADER_WHITTED || o->shader == MRT_SHADER_PATHTRACER || o->shader == MRT_SHADER_NOSHADOWS)) ||
+        o->width < 16 || o->height < 16 || (cam->kind != MRT_CAMERA_PERSPECTIVE && cam->kind != MRT_CAMERA_ORTHOGRAPHIC) || o->pixel_sampler < 0 ||
         o->pixel_sampler > 3 || o->light_sampler < 0 || o->light_sampler > 3 || o->rr_sampler < 0 || o->rr_sampler > 3) {
         set_error(ctx, "mrt_render_noalloc: invalid options");
         return MRT_ERR_ARG;
@@ -768,6 +771,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
     p.inv_h = 1.0f / (float)o->height;
     p.pw = 0.5f / (float)o->width;
     p.ph = 0.5f / (float)o->height;
+    p.depth_point = V3{o->depth_point[0], o->depth_point[1], o->depth_point[2]};
     p.tasks = nullptr;
     p.n_tasks = o->width * 16u * bsy;
     uint32_t *counters = reinterpret_cast<uint32_t *>(scratch + kNaCounters);
@@ -776,7 +780,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
     uint64_t rays_closest = 0, rays_shadow = 0;
     s->progress.store(0);
     cudaEventRecord(ctx->ev0, q);
-    if (o->shader == MRT_SHADER_NOSHADOWS) {
+    if (direct_shader(o->shader)) {
         if (accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST) {
             const uint32_t tiles_x = ((16u * bsy) % 4u == 0) ? o->width / 8u : 0u;
             cudaMemsetAsync(counters, 0, sizeof(uint32_t), q);

@@ -28,7 +28,13 @@ struct RenderParams {
     uint32_t *bitmap;
     float4 *accum;
     float inv_w, inv_h, pw, ph;
+    V3 depth_point;        // DepthMap maxPoint
 };
+
+// the shaders without secondary rays: the value is final at the camera ray
+MRT_HD bool direct_shader(int shader) {
+    return shader == MRT_SHADER_NOSHADOWS || shader == MRT_SHADER_DEPTHMAP || shader == MRT_SHADER_DIFFUSE;
+}
 
 __device__ __forceinline__ Task task_of(const RenderParams &p, uint32_t t) {
     if (p.tasks) return p.tasks[t];
@@ -98,6 +104,33 @@ __device__ __forceinline__ V3 shade_noshadows(const DevScene &s, const RenderPar
         rgb = rgb / (float)p.spl;
     }
     return rgb + kd * 0.1f;
+}
+
+// DepthMap::shade, DepthMap.cpp:19-26
+__device__ __forceinline__ V3 shade_depthmap(const RenderParams &p, const Ray &r, const Isect &it) {
+    const float max_dist = length(p.depth_point - r.o) * 2.0f;
+    const float x = (max_dist - it.length) / max_dist;
+    const float depth = x < 0.0f ? 0.0f : x;   // std::max(x, 0)
+    return V3{depth, depth, depth};
+}
+
+// DiffuseMaterial::shade, DiffuseMaterial.cpp:16-38
+__device__ __forceinline__ V3 shade_diffuse(const DevScene &s, const Isect &it) {
+    DevMaterial m;
+    if (!material_of(s, it, m)) return it.color;
+    if (any_pos(m.kd)) return m.kd;
+    if (any_pos(m.ks)) return m.ks;
+    if (any_pos(m.kt)) return m.kt;
+    if (any_pos(m.le)) return m.le;
+    return V3{0.0f, 0.0f, 0.0f};
+}
+
+// the value of a camera ray's hit under NoShadows, DepthMap or DiffuseMaterial
+__device__ __forceinline__ V3 shade_direct(const DevScene &s, const RenderParams &p, const Stream &st, const Ray &r,
+                                           const Isect &it) {
+    if (p.shader == MRT_SHADER_DEPTHMAP) return shade_depthmap(p, r, it);
+    if (p.shader == MRT_SHADER_DIFFUSE) return shade_diffuse(s, it);
+    return shade_noshadows(s, p, st, it, 1u);
 }
 
 

@@ -146,6 +146,13 @@ def camera(position, look_at, up=(0.0, 1.0, 0.0), fov_h=45.0, fov_v=45.0) -> cap
     return c
 
 
+def orthographic(position, look_at, up=(0.0, 1.0, 0.0), size_h=2.0, size_v=2.0) -> capi.MrtCamera:
+    """Components::Orthographic(position, lookAt, up, sizeH, sizeV) (Orthographic.cpp:12-17)."""
+    c = camera(position, look_at, up, size_h, size_v)
+    c.kind = capi.MRT_CAMERA_ORTHOGRAPHIC
+    return c
+
+
 def cli_camera(width: int, height: int) -> capi.MrtCamera:
     """The Linux CLI's default camera (c_wrapper.cpp:56-67): eye (0,0,-3.4) looking at +z,
     45 degrees scaled by the aspect ratio on the wider axis (float32 products, as there)."""

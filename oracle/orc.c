@@ -903,6 +903,11 @@ void orc_scene_destroy(OrcScene *s) {
 
 /* Shader::initializeAccelerators  Shader.cpp:31-122 */
 int orc_scene_build(OrcScene *s, int accel, int grid_size, int grid_index_mode, const float *cam) {
+    return orc_scene_build_box(s, accel, grid_size, grid_index_mode, cam, cam);
+}
+
+int orc_scene_build_box(OrcScene *s, int accel, int grid_size, int grid_index_mode, const float *cam_min,
+                        const float *cam_max) {
     scene_free_accel(s);
     s->accel = accel;
     for (int k = 0; k < 3; ++k) {
@@ -916,9 +921,8 @@ int orc_scene_build(OrcScene *s, int accel, int grid_size, int grid_index_mode, 
                 mn = vmin(b.mn, mn);
                 mx = vmax(b.mx, mx);
             }
-            const V3 c = vld(cam);   /* Camera::getAABB  Camera.cpp:39-44 */
-            mn = vmin(c, mn);
-            mx = vmax(c, mx);
+            mn = vmin(vld(cam_min), mn);   /* the camera's getAABB (AABBbounds, Scene.cpp:42-45) */
+            mx = vmax(vld(cam_max), mx);
             Box bounds; bounds.mn = vsubs(mn, EPS); bounds.mx = vadds(mx, EPS);
             int32_t G = grid_size_rule(ps->n);
             if (k == T_TRI && grid_size > 0) G = grid_size;
@@ -1122,13 +1126,19 @@ static V3 hemisphere(V3 n, float u1, float u2) {
 }
 
 /* ============================== camera  Camera.cpp:52-57, Perspective.cpp:10-44 =============== */
-typedef struct { V3 position, direction, right, up; float hfov, vfov; } Cam;
+typedef struct { V3 position, direction, right, up; float hfov, vfov; int kind; } Cam;
 static Cam cam_make(const MrtCamera *c) {
     Cam k;
     k.position = vld(c->position);
     k.direction = vnormalize(vsub(vld(c->look_at), k.position));
     k.right = vcross(vld(c->up), k.direction);
     k.up = vcross(k.direction, k.right);
+    k.kind = c->kind;
+    if (c->kind == MRT_CAMERA_ORTHOGRAPHIC) {   /* Orthographic.cpp:12-17 */
+        k.hfov = c->fov_h_deg / 2.0f;
+        k.vfov = c->fov_v_deg / 2.0f;
+        return k;
+    }
     const float pi = 3.14159265358979323846f;
     k.hfov = (c->fov_h_deg * pi) / 180.0f;
     k.vfov = (c->fov_v_deg * pi) / 180.0f;
@@ -1139,6 +1149,12 @@ static float fast_arctan(float x) {
     return 0.785398163397448309616f * x - (x * (ax - 1.0f)) * (0.2447f + (0.0663f * ax));
 }
 static Ray cam_ray(const Cam *k, float u, float v, float du, float dv) {
+    if (k->kind == MRT_CAMERA_ORTHOGRAPHIC) {   /* Orthographic::generateRay  Orthographic.cpp:23-34 */
+        const V3 right = vadd(vscale(k->right, (u - 0.5f) * k->hfov), vscale(k->right, du));
+        const V3 up = vadd(vscale(k->up, (0.5f - v) * k->vfov), vscale(k->up, dv));
+        Ray r; r.dir = k->direction; r.origin = vadd(vadd(k->position, right), up); r.depth = 1; r.exclude = MRT_HIT_NONE;
+        return r;
+    }
     const float rf = fast_arctan(k->hfov * (u - 0.5f)) + du;
     const V3 right = vscale(k->right, rf);
     const float uf = fast_arctan(k->vfov * (0.5f - v)) + dv;
@@ -1147,6 +1163,20 @@ static Ray cam_ray(const Cam *k, float u, float v, float du, float dv) {
     Ray r; r.dir = vnormalize(vsub(dest, k->position)); r.origin = k->position; r.depth = 1; r.exclude = MRT_HIT_NONE;
     return r;
 }
+/* Camera::getAABB (Camera.cpp:39-44) / Orthographic::getAABB (Orthographic.cpp:36-46) */
+void orc_camera_box(const MrtCamera *c, float *mn, float *mx) {
+    const Cam k = cam_make(c);
+    V3 a = k.position, b = k.position;
+    if (c->kind == MRT_CAMERA_ORTHOGRAPHIC) {
+        a = vadd(vadd(vadd(vadd(k.position, vscale(vscale(k.right, 0.0f - 0.5f), k.hfov)), vscale(k.right, -0.5f)),
+                      vscale(vscale(k.up, 0.5f - 0.0f), k.vfov)), vscale(k.up, -0.5f));
+        b = vadd(vadd(vadd(vadd(k.position, vscale(vscale(k.right, 1.0f - 0.5f), k.hfov)), vscale(k.right, 0.5f)),
+                      vscale(vscale(k.up, 0.5f - 1.0f), k.vfov)), vscale(k.up, 0.5f));
+    }
+    mn[0] = a.x; mn[1] = a.y; mn[2] = a.z;
+    mx[0] = b.x; mx[1] = b.y; mx[2] = b.z;
+}
+
 void orc_camera_ray(const MrtCamera *c, float u, float v, float du, float dv, float *o6) {
     const Cam k = cam_make(c);
     const Ray r = cam_ray(&k, u, v, du, dv);
@@ -1317,11 +1347,36 @@ static int shade_pathtracer(Ctx *c, V3 *rgb, const Isect *it, const Ray *r, uint
 }
 
 /* Shader::rayTrace  Shader.cpp:124-160 */
+/* DepthMap::shade  DepthMap.cpp:19-26 */
+static int shade_depthmap(Ctx *c, V3 *rgb, const Isect *it, const Ray *r) {
+    const float max_dist = vlength(vsub(vld(c->st->o->depth_point), r->origin)) * 2.0f;
+    const float x = (max_dist - it->length) / max_dist;
+    const float depth = x < 0.0f ? 0.0f : x;   /* std::max(x, 0.0f) */
+    *rgb = v3(depth, depth, depth);
+    return 0;
+}
+
+/* DiffuseMaterial::shade  DiffuseMaterial.cpp:16-38 */
+static int shade_diffuse(Ctx *c, V3 *rgb, const Isect *it) {
+    Mat m;
+    if (material_of(c->s, it, &m)) {
+        if (vany_pos(m.kd)) *rgb = m.kd;
+        else if (vany_pos(m.ks)) *rgb = m.ks;
+        else if (vany_pos(m.kt)) *rgb = m.kt;
+        else if (vany_pos(m.le)) *rgb = m.le;
+    } else {
+        *rgb = it->color;
+    }
+    return 0;
+}
+
 static int ray_trace(Ctx *c, V3 *rgb, const Ray *r, uint32_t node) {
     Isect it;
     c->st->n_closest++;
     if (!scene_closest(c->s, r, &it)) return 0;
     switch (c->st->o->shader) {
+        case MRT_SHADER_DEPTHMAP: return shade_depthmap(c, rgb, &it, r);
+        case MRT_SHADER_DIFFUSE: return shade_diffuse(c, rgb, &it);
         case MRT_SHADER_WHITTED: return shade_whitted(c, rgb, &it, r, node);
         case MRT_SHADER_PATHTRACER: return shade_pathtracer(c, rgb, &it, r, node);
         default: return shade_noshadows(c, rgb, &it, node);

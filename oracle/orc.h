@@ -36,6 +36,10 @@ OrcScene *orc_scene_create(const MrtSceneDesc *desc);
 void orc_scene_destroy(OrcScene *s);
 /* accel: ORC_ACCEL_*; grid_size 0 = reference rule; grid_index MRT_GRID_INDEX_* */
 int orc_scene_build(OrcScene *s, int accel, int grid_size, int grid_index, const float *camera_position);
+/* grid bounds including the camera box [camera_min, camera_max] (orc_camera_box) */
+int orc_scene_build_box(OrcScene *s, int accel, int grid_size, int grid_index, const float *camera_min,
+                        const float *camera_max);
+void orc_camera_box(const MrtCamera *c, float *mn, float *mx);
 int orc_scene_grid_size(const OrcScene *s, int type);
 uint64_t orc_scene_bvh_nodes(const OrcScene *s, int type);
 

@@ -38,6 +38,8 @@ def orc() -> ctypes.CDLL:
             "orc_scene_create": (vp, [vp]),
             "orc_scene_destroy": (None, [vp]),
             "orc_scene_build": (ip, [vp, ip, ip, ip, fp]),
+            "orc_scene_build_box": (ip, [vp, ip, ip, ip, fp, fp]),
+            "orc_camera_box": (None, [vp, fp, fp]),
             "orc_scene_grid_size": (ip, [vp, ip]),
             "orc_scene_bvh_nodes": (ctypes.c_uint64, [vp, ip]),
             "orc_trace_closest": (None, [vp, vp, ctypes.c_uint32, vp, ip]),
@@ -125,15 +127,23 @@ def make_rays(origins: np.ndarray, dirs: np.ndarray, depth: int = 1, exclude=Non
 class OrcScene:
     """The restatement's scene with one accelerator built."""
 
-    def __init__(self, scene, accel: int, grid_size: int = 0, grid_index: int = 0, camera_position=None):
+    def __init__(self, scene, accel: int, grid_size: int = 0, grid_index: int = 0, camera_position=None,
+                 camera=None):
+        """Grid bounds include `camera`'s getAABB, else the point `camera_position`, else the
+        scene's own camera (as Scene.build on the device side)."""
         self.lib = orc()
         self._scene = scene
         self._desc = scene.desc()
         self.h = self.lib.orc_scene_create(ctypes.byref(self._desc))
-        cam = camera_position if camera_position is not None else (
-            list(scene.camera.position) if scene.camera is not None else [0.0, 0.0, 0.0])
-        self._cam = f32(*cam)
-        self.lib.orc_scene_build(self.h, accel, grid_size, grid_index, fptr(self._cam))
+        if camera is None and camera_position is None and scene.camera is not None:
+            camera = scene.camera
+        if camera is not None:
+            self._cmin, self._cmax = f32(0, 0, 0), f32(0, 0, 0)
+            self.lib.orc_camera_box(ctypes.byref(camera), fptr(self._cmin), fptr(self._cmax))
+            self.lib.orc_scene_build_box(self.h, accel, grid_size, grid_index, fptr(self._cmin), fptr(self._cmax))
+        else:
+            self._cam = f32(*(camera_position if camera_position is not None else [0.0, 0.0, 0.0]))
+            self.lib.orc_scene_build(self.h, accel, grid_size, grid_index, fptr(self._cam))
 
     def close(self):
         if self.h:

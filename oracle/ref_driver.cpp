@@ -11,6 +11,7 @@
 // Scenes arrive in the mrt_cuda.h MrtSceneDesc layout so the same arrays feed the CUDA path.
 #include "../include/mrt_cuda.h"
 
+#include "Components/Cameras/Orthographic.hpp"
 #include "Components/Cameras/Perspective.hpp"
 #include "Components/Lights/AreaLight.hpp"
 #include "Components/Lights/PointLight.hpp"
@@ -18,6 +19,8 @@
 #include "Components/Samplers/HaltonSeq.hpp"
 #include "Components/Samplers/MersenneTwister.hpp"
 #include "Components/Samplers/Stratified.hpp"
+#include "Components/Shaders/DepthMap.hpp"
+#include "Components/Shaders/DiffuseMaterial.hpp"
 #include "Components/Shaders/NoShadows.hpp"
 #include "Components/Shaders/PathTracer.hpp"
 #include "Components/Shaders/Whitted.hpp"
@@ -136,7 +139,7 @@ template <> const Sphere *storage<Sphere>(const Shader &s, int a) {
 
 struct TraceHandle {
     std::unique_ptr<IdShader> shader;
-    std::unique_ptr<::Components::Perspective> camera;
+    std::unique_ptr<::MobileRT::Camera> camera;
     int accel;
     uint32_t n_tri, n_sph, n_pln, n_lights;
 };
@@ -213,11 +216,17 @@ std::unique_ptr<Shader> make_shader(Scene &&scene, const MrtRenderOpts &o, int a
         case MRT_SHADER_PATHTRACER:
             return std::make_unique<::Components::PathTracer>(
                 std::move(scene), make_sampler(o.rr_sampler, o.constant_value, o.width, o.height, o.spp), o.spl, a);
+        case MRT_SHADER_DEPTHMAP:
+            return std::make_unique<::Components::DepthMap>(std::move(scene), v3(o.depth_point), a);
+        case MRT_SHADER_DIFFUSE: return std::make_unique<::Components::DiffuseMaterial>(std::move(scene), a);
         default: return std::make_unique<::Components::NoShadows>(std::move(scene), o.spl, a);
     }
 }
 
-std::unique_ptr<::Components::Perspective> make_camera(const MrtCamera &c) {
+std::unique_ptr<::MobileRT::Camera> make_camera(const MrtCamera &c) {
+    if (c.kind == MRT_CAMERA_ORTHOGRAPHIC)
+        return std::make_unique<::Components::Orthographic>(v3(c.position), v3(c.look_at), v3(c.up), c.fov_h_deg,
+                                                             c.fov_v_deg);
     return std::make_unique<::Components::Perspective>(v3(c.position), v3(c.look_at), v3(c.up), c.fov_h_deg, c.fov_v_deg);
 }
 

@@ -39,6 +39,10 @@ def job_list():
                                          rr_sampler=R, depth_min=2, depth_max=5, seed=9, spp_offset=4), 3, True),
         (gr, gr.camera, capi.render_opts(shader=WH, width=64, height=48, spp=2, spl=3, seed=2), None, False),
         (soup, soup.camera, capi.render_opts(shader=PT, width=64, height=64, spp=1, seed=8), None, True),
+        (gr, scenes.orthographic((0.3, 0.2, -3.4), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 2.6, 1.9),
+         capi.render_opts(shader=capi.MRT_SHADER_DEPTHMAP, width=64, height=48, spp=2, seed=5,
+                          depth_point=(1.5, 1.0, 2.0)), None, True),
+        (cb, cb.camera, capi.render_opts(shader=capi.MRT_SHADER_DIFFUSE, width=48, height=32, spp=3, seed=6), None, True),
     ]
     return jobs
 

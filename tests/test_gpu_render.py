@@ -142,3 +142,22 @@ def test_errors_are_reported(ctx):
         g.render(sc.camera, bad)
     ok, _, _ = g.render(sc.camera, capi.render_opts(width=32, height=32))   # context still usable
     assert ok.any()
+
+
+@pytest.mark.parametrize("shader", [capi.MRT_SHADER_DEPTHMAP, capi.MRT_SHADER_DIFFUSE, NS])
+@pytest.mark.parametrize("ortho", [False, True])
+@pytest.mark.parametrize("accel,mode,oacc", GPU_ACCELS)
+def test_depthmap_diffuse_orthographic(ctx, shader, ortho, accel, mode, oacc):
+    """DepthMap (DepthMap.cpp:19-26) and DiffuseMaterial (DiffuseMaterial.cpp:16-38) frames, and the
+    Orthographic camera (Orthographic.cpp:23-46, including its film rectangle in the grid bounds)."""
+    sc = scenes.glass_room()
+    cam = scenes.orthographic((0.3, 0.2, -3.4), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 2.6, 1.9) if ortho else sc.camera
+    sc.camera = cam
+    opts = capi.render_opts(shader=shader, width=96, height=64, spp=2, spl=1, seed=3, depth_point=(1.5, 1.0, 2.0),
+                            pixel_sampler=capi.MRT_SAMPLER_STRATIFIED)
+    g = Scene(ctx, sc).build(accel, mode, camera=cam)
+    bm_g, acc_g, stats = g.render(cam, opts, accum=np.zeros((opts.height, opts.width, 4), np.float32))
+    bm_o, acc_o, counts = O.OrcScene(sc, oacc, camera=cam).render(cam, opts)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-4)
+    assert stats.rays_closest == counts[0]
+    assert np.count_nonzero(bm_g & 0xFFFFFF) > 1000

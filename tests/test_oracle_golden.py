@@ -130,6 +130,27 @@ def test_restatement_equals_reference_frames():
 
 
 @pytest.mark.skipif(not _ref_available(), reason="compiled reference not built (make -C oracle ref)")
+def test_restatement_equals_reference_depthmap_diffuse_orthographic():
+    """DepthMap and DiffuseMaterial frames, and every direct shader through an Orthographic camera
+    (whose film rectangle also widens the grid bounds, Orthographic.cpp:36-46), on every accelerator."""
+    ortho = scenes.orthographic((0.3, 0.2, -3.4), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 2.6, 1.9)
+    for sc in (scenes.glass_room(), scenes.cornell_box(), scenes.triangle_soup(5000, 2, 96, 64)):
+        sc.lights = [scenes.point_light((0.1, 0.45, -0.3))]
+        for cam in (sc.camera, ortho):
+            for shader in (0, 3, 4):
+                for accel in (0, 1, 2):
+                    if shader == 0 and cam is sc.camera:
+                        continue   # covered above
+                    opts = capi.render_opts(shader=shader, width=96, height=64, spp=1, spl=1,
+                                            depth_point=(1.5, 1.0, 2.0))
+                    sc.camera = cam
+                    bm_r, _, _ = O.ref_render(sc, cam, opts, accel, threads=4)
+                    bm_o, _, _ = O.OrcScene(sc, accel).render(cam, opts, threads=4)
+                    assert (bm_r == bm_o).all(), (shader, accel, cam.kind)
+                    assert np.count_nonzero(bm_o & 0xFFFFFF) > 20
+
+
+@pytest.mark.skipif(not _ref_available(), reason="compiled reference not built (make -C oracle ref)")
 def test_restatement_scalar_functions():
     ref, orc = O.ref(), O.orc()
     for i in range(300):
