@@ -9,6 +9,8 @@
  *   mrt_scene_create      Scene{triangles_, spheres_, planes_, materials_, lights_} filled by the caller
  *                         (app/MobileRT/Scene.hpp:23-27, filled in app/Scenes/Scenes.cpp:7-314 or
  *                         app/Components/ObjectLoaders/OBJLoader.cpp:68-248)
+ *   mrt_obj_load          OBJLoader::process + OBJLoader::fillScene
+ *                         (app/Components/ObjectLoaders/OBJLoader.cpp:21-248)
  *   mrt_scene_build       Shader::initializeAccelerators(Camera*)   (app/MobileRT/Shader.cpp:31-122)
  *                         -> Naive<T>, RegularGrid<T>, BVH<T> constructors
  *   mrt_trace_closest     Shader::rayTrace's accelerator part: planes -> spheres -> triangles -> lights
@@ -246,6 +248,19 @@ int mrt_scene_move(MrtScene *scene, MrtContext *ctx);
 uint64_t mrt_scene_device_bytes(const MrtScene *scene);
 /* Accelerator statistics: nodes (BVH records) or cells (grid), references, grid size. */
 int mrt_scene_accel_info(const MrtScene *scene, uint64_t *nodes, uint64_t *refs, int32_t *grid_size);
+
+/* ---- scene files ---------------------------------------------------------------------------- */
+/* OBJLoader::process + fillScene (app/Components/ObjectLoaders/OBJLoader.cpp:21-248): reads a
+ * Wavefront OBJ and the MTL file the caller names (mtl_path may be NULL: no materials) and fills
+ * *desc with the scene the reference loader would build: x negated, polygons split as fans, given
+ * normals normalised (else the Triangle constructor's normal), vertex colours, Ks / 2,
+ * Kt * (1 - d), emission scaled down to a largest component of 1, emitting faces as AreaLights,
+ * equal materials merged.  *desc points into *out until mrt_obj_free(*out).  On failure returns
+ * MRT_ERR_ARG with the reason in error[0 .. error_len). */
+typedef struct MrtObjScene MrtObjScene;
+int mrt_obj_load(const char *obj_path, const char *mtl_path, MrtObjScene **out, MrtSceneDesc *desc, char *error,
+                 size_t error_len);
+void mrt_obj_free(MrtObjScene *scene);
 
 /* ---- traversal ------------------------------------------------------------------------------ */
 int mrt_trace_closest(MrtScene *scene, const MrtRay *rays, uint32_t n, MrtHit *hits, uint32_t mem);

@@ -181,6 +181,9 @@ def load() -> ctypes.CDLL:
         "mrt_arena_stats": (ctypes.c_int, [vp, P(ctypes.c_uint64), P(ctypes.c_uint64), P(ctypes.c_uint64),
                                            P(ctypes.c_uint64)]),
         "mrt_context_set_arena": (ctypes.c_int, [vp, vp]),
+        "mrt_obj_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(vp), P(MrtSceneDesc), ctypes.c_char_p,
+                                        ctypes.c_size_t]),
+        "mrt_obj_free": (None, [vp]),
         "mrt_render_stop": (None, [vp]),
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
     }
@@ -199,4 +202,5 @@ EXPORTED_SYMBOLS = [
     "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress", "mrt_batch_create", "mrt_batch_destroy",
     "mrt_batch_submit", "mrt_batch_step", "mrt_batch_completed", "mrt_batch_run", "mrt_batch_stats",
     "mrt_arena_create", "mrt_arena_destroy", "mrt_arena_stats", "mrt_context_set_arena", "mrt_scene_move",
+    "mrt_obj_load", "mrt_obj_free",
 ]

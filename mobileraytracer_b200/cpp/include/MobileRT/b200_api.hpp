@@ -22,6 +22,7 @@
 #include <glm/glm.hpp>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -357,6 +358,29 @@ public:
     explicit DiffuseMaterial(::MobileRT::Scene &&scene, Accelerator accelerator) noexcept
         : Shader{std::move(scene), 0, accelerator} {}
     int shaderKind() const noexcept final { return 4; }
+};
+
+// OBJLoader.hpp: reads a Wavefront OBJ and the named MTL file with the reference loader's conventions
+// (OBJLoader.cpp:21-248) through the library's parser (mrt_obj_load).
+class OBJLoader final {
+public:
+    explicit OBJLoader(std::string obj, std::string materials) noexcept;
+    OBJLoader(const OBJLoader &) = delete;
+    OBJLoader &operator=(const OBJLoader &) = delete;
+    ~OBJLoader() noexcept;
+    // number of triangles (emitting faces included), -1 when the files cannot be read
+    std::int32_t process() noexcept;
+    // appends the triangles, materials and area lights (each light sampler from `lambda`)
+    bool fillScene(::MobileRT::Scene *scene, std::function<std::unique_ptr<::MobileRT::Sampler>()> lambda) noexcept;
+    bool isProcessed() const noexcept { return isProcessed_; }
+    const std::string &lastError() const noexcept { return error_; }
+
+private:
+    std::string objFilePath_{}, mtlFilePath_{};
+    void *data_{nullptr};
+    bool isProcessed_{false};
+    std::int32_t numberTriangles_{-1};
+    std::string error_{};
 };
 
 }  // namespace Components

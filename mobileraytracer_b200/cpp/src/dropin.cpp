@@ -209,3 +209,56 @@ std::uint32_t Renderer::getSample() const noexcept {
 }
 
 }  // namespace MobileRT
+
+namespace Components {
+
+namespace {
+struct ObjData {
+    MrtObjScene *scene{nullptr};
+    MrtSceneDesc desc{};
+    ~ObjData() { if (scene) mrt_obj_free(scene); }
+};
+}  // namespace
+
+OBJLoader::OBJLoader(std::string obj, std::string materials) noexcept
+    : objFilePath_{std::move(obj)}, mtlFilePath_{std::move(materials)} {}
+
+OBJLoader::~OBJLoader() noexcept { delete static_cast<ObjData *>(data_); }
+
+std::int32_t OBJLoader::process() noexcept {
+    delete static_cast<ObjData *>(data_);
+    ObjData *o = new ObjData();
+    data_ = o;
+    char err[512] = {0};
+    const int st = mrt_obj_load(objFilePath_.c_str(), mtlFilePath_.empty() ? nullptr : mtlFilePath_.c_str(), &o->scene,
+                                &o->desc, err, sizeof(err));
+    isProcessed_ = st == MRT_OK;
+    error_ = isProcessed_ ? std::string{} : std::string{err};
+    numberTriangles_ = isProcessed_ ? (std::int32_t)(o->desc.n_triangles + o->desc.n_lights) : -1;
+    return numberTriangles_;
+}
+
+bool OBJLoader::fillScene(::MobileRT::Scene *scene, std::function<std::unique_ptr<::MobileRT::Sampler>()> lambda) noexcept {
+    if (!isProcessed_ || !data_ || !scene) return false;
+    const MrtSceneDesc &d = static_cast<ObjData *>(data_)->desc;
+    auto v = [](const float *p) { return ::glm::vec3{p[0], p[1], p[2]}; };
+    auto mat = [&](const MrtMaterial &m) {
+        return ::MobileRT::Material{v(m.kd), v(m.ks), v(m.kt), m.ior, v(m.le)};
+    };
+    const std::size_t m0 = scene->materials_.size();
+    for (std::uint32_t i = 0; i < d.n_materials; ++i) scene->materials_.emplace_back(mat(d.materials[i]));
+    scene->triangles_.reserve(scene->triangles_.size() + d.n_triangles);
+    for (std::uint32_t i = 0; i < d.n_triangles; ++i) {
+        const float *p = d.tri_abc + 9 * (std::size_t)i, *n = d.tri_normals + 9 * (std::size_t)i,
+                    *c = d.tri_colors + 9 * (std::size_t)i;
+        const std::int32_t m = d.tri_material[i] < 0 ? -1 : d.tri_material[i] + (std::int32_t)m0;
+        scene->triangles_.emplace_back(v(p), v(p + 3), v(p + 6), m, v(n), v(n + 3), v(n + 6), v(c), v(c + 3), v(c + 6));
+    }
+    for (std::uint32_t i = 0; i < d.n_lights; ++i) {
+        const MrtLightDesc &l = d.lights[i];
+        scene->lights_.emplace_back(std::make_unique<AreaLight>(mat(l.radiance), lambda(), v(l.p0), v(l.p1), v(l.p2)));
+    }
+    return true;
+}
+
+}  // namespace Components

@@ -364,6 +364,39 @@ def batched_jobs(count: int = 256, n_min: float = 1e3, n_max: float = 2e6, side_
     return jobs
 
 
+def load_obj(obj_path: str, mtl_path: str | None = None, camera: capi.MrtCamera | None = None) -> Scene:
+    """A scene from a Wavefront OBJ (and the MTL file named here) through the library's loader,
+    mrt_obj_load (the reference's OBJLoader conventions); the arrays are copied into numpy."""
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    d = capi.MrtSceneDesc()
+    err = ctypes.create_string_buffer(512)
+    st = lib.mrt_obj_load(obj_path.encode(), mtl_path.encode() if mtl_path else None, ctypes.byref(h),
+                          ctypes.byref(d), err, len(err))
+    if st != capi.MRT_OK:
+        from . import MrtError
+        raise MrtError(st, err.value.decode(errors="replace"))
+    try:
+        n = d.n_triangles
+        s = Scene()
+
+        def arr(ptr, count, dtype):
+            if count == 0 or not ptr:
+                return np.zeros(count, dtype)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype).copy()
+
+        s.tri_abc = arr(d.tri_abc, 9 * n, np.float32).reshape(n, 9)
+        s.tri_normals = arr(d.tri_normals, 9 * n, np.float32).reshape(n, 9)
+        s.tri_colors = arr(d.tri_colors, 9 * n, np.float32).reshape(n, 9)
+        s.tri_material = arr(d.tri_material, n, np.int32)
+        s.materials = [capi.MrtMaterial.from_buffer_copy(d.materials[i]) for i in range(d.n_materials)]
+        s.lights = [capi.MrtLightDesc.from_buffer_copy(d.lights[i]) for i in range(d.n_lights)]
+        s.camera = camera
+        return s
+    finally:
+        lib.mrt_obj_free(h)
+
+
 def glass_room() -> Scene:
     """Every primitive type and material branch: 6 planes (a closed room), a mirror sphere, a glass
     sphere (ior 1.9), a diffuse+specular sphere, two coloured triangles with given normals and

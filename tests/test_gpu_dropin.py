@@ -83,3 +83,36 @@ def test_renderframe_through_the_dropin(ctx, client, tmp_path, shader, accel, mo
         got = np.fromfile(out, np.uint32).reshape(48, 80)
         want, _, _ = Scene(ctx, sc).build(accel, mode).render(sc.camera, opts)
         assert (got == want).all()
+
+
+@pytest.fixture(scope="module")
+def obj_client(tmp_path_factory):
+    build_dropin()
+    exe = str(tmp_path_factory.mktemp("dropin_obj") / "dropin_obj")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", "-I", os.path.join(HERE, "cpp", "include"), "-I",
+                    os.path.join(HERE, "cpp", "glm_min"), os.path.join(ROOT, "tests", "cpp", "dropin_obj.cpp"),
+                    "-L", os.path.dirname(DROPIN_OUT), "-lmrt_dropin", "-lmrt_cuda",
+                    "-Wl,-rpath," + os.path.dirname(DROPIN_OUT), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("shader,ortho", [(capi.MRT_SHADER_WHITTED, 0), (capi.MRT_SHADER_DEPTHMAP, 1),
+                                          (capi.MRT_SHADER_DIFFUSE, 0)])
+def test_obj_scene_through_the_dropin(ctx, obj_client, tmp_path, shader, ortho):
+    """Components::OBJLoader + DepthMap / DiffuseMaterial / Orthographic through the drop-in: equal to
+    the C ABI render of the scene mrt_obj_load reads."""
+    obj = os.path.join(ROOT, "tests", "golden", "obj", "room.obj")
+    mtl = os.path.join(ROOT, "tests", "golden", "obj", "room.mtl")
+    out = str(tmp_path / "out.bin")
+    r = subprocess.run([obj_client, obj, mtl, str(shader), str(ortho), "64", "48", out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, np.uint32).reshape(48, 64)
+    if ortho:
+        cam = scenes.orthographic((0.0, 0.1, -2.6), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 2.4, 2.0)
+    else:
+        cam = scenes.camera((0.0, 0.1, -2.6), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 55.0, 55.0)
+    sc = scenes.load_obj(obj, mtl, camera=cam)
+    opts = capi.render_opts(shader=shader, width=64, height=48, spp=1, spl=1, depth_point=(1.5, 1.0, 2.0))
+    want, _, _ = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST, camera=cam).render(cam, opts)
+    assert (got == want).all()
+    assert np.count_nonzero(want & 0xFFFFFF) > 500
