@@ -43,6 +43,7 @@ struct MrtContext {
     int32_t *d_error = nullptr;         // device error flag (MRT_ERR_LIMIT from kernels)
     uint32_t *d_counters = nullptr;     // work counters of the persistent kernels (64 slots)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t wave_ev[2] = {nullptr, nullptr};   // the last two waves of a render (bounded run-ahead)
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];
     MrtArena *arena = nullptr;          // device allocations of this context come from here when set

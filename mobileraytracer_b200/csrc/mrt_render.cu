@@ -448,6 +448,14 @@ void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState
         else fn<MRT_ACCEL_BVH, MRT_BVH_FAST>(__VA_ARGS__);                                                  \
     } while (0)
 
+// Renderer::stopRender seen between waves: the work already queued finishes (the caller's buffers
+// stay in use until then), the bitmap keeps the samples folded so far
+int cancelled(MrtContext *ctx, cudaStream_t q) {
+    cudaStreamSynchronize(q);
+    set_error(ctx, "render stopped (mrt_render_stop)");
+    return MRT_ERR_CANCELLED;
+}
+
 uint32_t wave_roots_setting() {
     static uint32_t v = [] {
         const char *e = getenv("MRT_WAVE_ROOTS");
@@ -528,7 +536,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         const uint32_t rows = 16u * (o->height / 16u);
         const uint32_t tiles_x = (plan.implicit && o->width % 8u == 0 && rows % 4u == 0) ? o->width / 8u : 0u;
         for (size_t r = 0; r < plan.round_first.size(); ++r) {
-            if (s->stop.load()) return MRT_ERR_CANCELLED;
+            if (s->stop.load()) return cancelled(ctx, q);
             if (fast) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
@@ -565,11 +573,21 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         w.ray_cap = (uint32_t)ray_cap;
         w.shadow_cap = (uint32_t)shadow_cap;
         cudaMemsetAsync(w.counters, 0, 16, q);
+        // at most one wave queued ahead of the one running: a stop request ends the render within two
+        // waves, and progress counts finished waves
+        uint64_t waves_issued = 0;
+        uint64_t done_samples[2] = {0, 0};
         for (size_t rd = 0; rd < plan.round_first.size(); ++rd) {
             p.task_base = plan.round_first[rd];
             const uint64_t total_roots = (uint64_t)plan.round_count[rd] * o->spp;
             for (uint64_t r0 = 0; r0 < total_roots; r0 += wave) {
-                if (s->stop.load()) return MRT_ERR_CANCELLED;
+                if (waves_issued >= 2) {
+                    const int slot = (int)(waves_issued % 2);
+                    st = cuda_status(ctx, cudaEventSynchronize(ctx->wave_ev[slot]), "render");
+                    if (st != MRT_OK) return st;
+                    s->progress.store((uint32_t)done_samples[slot]);
+                }
+                if (s->stop.load()) return cancelled(ctx, q);
                 w.root_first = (uint32_t)r0;
                 w.n_roots = (uint32_t)std::min<uint64_t>(wave, total_roots - r0);
                 cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
@@ -579,7 +597,10 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                     MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);
                 for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
                 k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
-                s->progress.store((uint32_t)((r0 + w.n_roots) / std::max<uint64_t>(1, plan.round_count[rd])));
+                const int slot = (int)(waves_issued % 2);
+                cudaEventRecord(ctx->wave_ev[slot], q);
+                done_samples[slot] = (r0 + w.n_roots) / std::max<uint64_t>(1, plan.round_count[rd]);
+                ++waves_issued;
             }
         }
         unsigned long long cnt[2] = {0, 0};
@@ -804,7 +825,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
         const uint64_t total_roots = (uint64_t)p.n_tasks * o->spp;
         p.task_base = 0;
         for (uint64_t r0 = 0; r0 < total_roots; r0 += kNoAllocWave) {
-            if (s->stop.load()) return MRT_ERR_CANCELLED;
+            if (s->stop.load()) return cancelled(ctx, q);
             w.root_first = (uint32_t)r0;
             w.n_roots = (uint32_t)std::min<uint64_t>(kNoAllocWave, total_roots - r0);
             cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);

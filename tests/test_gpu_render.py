@@ -161,3 +161,42 @@ def test_depthmap_diffuse_orthographic(ctx, shader, ortho, accel, mode, oacc):
     assert_same(bm_g, acc_g, bm_o, acc_o, 1e-4)
     assert stats.rays_closest == counts[0]
     assert np.count_nonzero(bm_g & 0xFFFFFF) > 1000
+
+
+def test_stop_and_progress(ctx):
+    """Renderer::stopRender from another thread while renderFrame runs (Renderer.cpp:61-65) and
+    getSample as progress (Renderer.cpp:118-120): the render returns MRT_ERR_CANCELLED after the
+    waves already queued, having reported progress, and the scene renders normally afterwards."""
+    import threading
+    import time
+    import torch
+    from mobileraytracer_b200 import MrtError
+    sc = scenes.cornell_box()
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
+    opts = capi.render_opts(shader=PT, width=512, height=512, spp=512, spl=1, depth_min=3, depth_max=6)
+    bm = torch.zeros(512 * 512, dtype=torch.int32, device="cuda")
+    box = {}
+
+    def run():
+        try:
+            g.render(sc.camera, opts, bitmap=bm)
+            box["status"] = capi.MRT_OK
+        except MrtError as e:
+            box["status"] = e.status
+
+    t = threading.Thread(target=run)
+    t.start()
+    seen = 0
+    t0 = time.time()
+    while t.is_alive() and time.time() - t0 < 60:
+        seen = max(seen, g.progress())
+        if seen > 0:
+            g.stop()
+            break
+        time.sleep(0.001)
+    t.join(120)
+    assert not t.is_alive()
+    assert box["status"] == capi.MRT_ERR_CANCELLED, box
+    assert 0 < seen < 512
+    small = capi.render_opts(shader=PT, width=64, height=64, spp=2, spl=1)
+    g.render(sc.camera, small)   # no error: the stop request was consumed
