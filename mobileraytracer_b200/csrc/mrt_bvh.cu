@@ -387,7 +387,8 @@ __device__ __forceinline__ void write_empty_slot(float4 *rec) {
 __global__ void k_collapse_root(const float4 *bin, float4 *wide, CollapseItem *queue, uint32_t *ctrs) {
     const float4 lo = bin[0], hi = bin[1];
     if (__float_as_int(hi.w) > 0) {
-        write_record(wide, lo, hi, __float_as_uint(lo.w), (uint32_t)__float_as_int(hi.w));
+        write_record(wide, lo, hi, leaf_code(__float_as_uint(lo.w), (uint32_t)__float_as_int(hi.w)),
+                     (uint32_t)__float_as_int(hi.w));
         for (int k = 1; k < kWide; ++k) write_empty_slot(wide + 2 * k);
         ctrs[0] = 0;   // next level: empty
     } else {
@@ -430,7 +431,7 @@ __global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, c
         if (k >= m) { write_empty_slot(node + 2 * k); continue; }
         const float4 lo = bin[2 * (size_t)rec[k]], hi = bin[2 * (size_t)rec[k] + 1];
         const int b = __float_as_int(hi.w);
-        if (b > 0) { write_record(node + 2 * k, lo, hi, __float_as_uint(lo.w), (uint32_t)b); continue; }
+        if (b > 0) { write_record(node + 2 * k, lo, hi, leaf_code(__float_as_uint(lo.w), (uint32_t)b), (uint32_t)b); continue; }
         const uint32_t a = __float_as_uint(lo.w);
         const uint32_t j = atomicAdd(&ctrs[1], 1u);
         const uint32_t q = atomicAdd(&ctrs[0], 1u);

@@ -26,6 +26,9 @@ constexpr uint32_t kMaxLeafFirst = 1u << 27;
 constexpr float kSphereEpsilon = 1.0e-05f;  // Sphere.cpp:43,50
 
 #define MRT_HD __host__ __device__ __forceinline__
+MRT_HD uint32_t leaf_code(uint32_t first, uint32_t count) { return kLeafCode | ((count - 1u) << 27) | first; }
+MRT_HD uint32_t code_first(uint32_t c) { return c & (kMaxLeafFirst - 1u); }
+MRT_HD uint32_t code_count(uint32_t c) { return ((c >> 27) & 15u) + 1u; }
 
 struct V3 {
     float x, y, z;

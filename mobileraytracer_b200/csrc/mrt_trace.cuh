@@ -402,11 +402,6 @@ __device__ __forceinline__ void fast_leaf(const S &s, const Ray &r, uint32_t fir
     }
 }
 
-__device__ __forceinline__ uint32_t leaf_code(uint32_t first, uint32_t count) {
-    return kLeafCode | ((count - 1u) << 27) | first;
-}
-__device__ __forceinline__ uint32_t code_first(uint32_t c) { return c & (kMaxLeafFirst - 1u); }
-__device__ __forceinline__ uint32_t code_count(uint32_t c) { return ((c >> 27) & 15u) + 1u; }
 
 __device__ __forceinline__ void cmp_swap(float (&t)[kWide], uint32_t (&c)[kWide], int i, int j) {
     const bool sw = t[j] < t[i];
@@ -419,7 +414,7 @@ __device__ __forceinline__ void cmp_swap(float (&t)[kWide], uint32_t (&c)[kWide]
 }
 
 // One node of the FAST tree: kWide child records {min.xyz, a}{max.xyz, b} (b = 0: internal child,
-// node a; b > 0: leaf of b triangles at a; b < 0: empty slot).  Returns the number of children the
+// node a; b > 0: leaf of b triangles, a = its leaf code; b < 0: empty slot).  Returns the number of children the
 // ray segment [0, tmax] may touch; with kSort their (entry distance, code) come first, nearest
 // first, the others follow at +inf.
 template <bool kSort, class S>
@@ -439,7 +434,7 @@ __device__ __forceinline__ int wide_children(const S &s, uint32_t node, const Fa
         float tn;
         const bool hit = fast_slab(lo[k], hi[k], f, tmax, tn) && b >= 0;
         t[k] = hit ? tn : __int_as_float(0x7f800000);
-        c[k] = b > 0 ? leaf_code(__float_as_uint(lo[k].w), (uint32_t)b) : __float_as_uint(lo[k].w);
+        c[k] = __float_as_uint(lo[k].w);   // node index, or the leaf code written by the build
         n += hit ? 1 : 0;
     }
     if (kSort) {
