@@ -332,6 +332,7 @@ def bench_batched(args):
                    "l2": "inputs (scenes ~GBs) far larger than L2",
                    "policy": args.policy, "wave_roots": st.wave_roots, "block_threads": st.block_threads,
                    "blocks_per_sm": st.blocks_per_sm, "pipelines": st.pipelines, "autotuner_probes": st.autotuned,
+                   "whole_path_waves": st.waves_paths,
                    "waves_per_step": st.waves / (args.warmup + args.steps),
                    "device_busy_fraction": b_busy / 1e3 / b_time},
         "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_step": p_time * 1e3 / args.steps,

@@ -318,7 +318,13 @@ typedef struct MrtBatchOpts {
     uint32_t policy;         /* MRT_BATCH_SMALLEST_FIRST (0), MRT_BATCH_FIFO or MRT_BATCH_EQUAL_SHARE */
     uint32_t pipelines;      /* waves in flight at once (1..4), each with its own stream and ray pool;
                                 0 = autotuner (buffers for 4 are allocated) */
+    uint32_t kernel;         /* MRT_BATCH_KERNEL_WAVEFRONT (one launch per bounce level),
+                                MRT_BATCH_KERNEL_PATHS (whole paths per lane, one launch), 0 = per
+                                wave: whole paths when no job holds half of the wave */
 } MrtBatchOpts;
+
+#define MRT_BATCH_KERNEL_WAVEFRONT 1
+#define MRT_BATCH_KERNEL_PATHS 2
 
 /* Which jobs fill a wave: the fewest paths left first / submission order / an equal share each. */
 #define MRT_BATCH_SMALLEST_FIRST 0
@@ -347,7 +353,8 @@ typedef struct MrtBatchStats {
     uint32_t blocks_per_sm;
     uint32_t autotuned;      /* candidates the autotuner timed (0: fixed settings) */
     uint32_t pipelines;
-    uint32_t reserved;
+    uint32_t kernel;         /* MRT_BATCH_KERNEL_* chosen for waves dominated by one job */
+    uint64_t waves_paths;    /* waves run as whole-path launches */
 } MrtBatchStats;
 
 int mrt_batch_create(MrtContext *ctx, const MrtBatchOpts *opts, MrtBatch **out);

@@ -234,7 +234,8 @@ class Batch:
 
     def __init__(self, ctx: Context, wave_roots: int = 0, block_threads: int = 0, blocks_per_sm: int = 0,
                  max_jobs: int = 0, max_depth: int = 0, max_spl: int = 0, graph: bool = True,
-                 max_wave_roots: int = 0, policy: int = capi.MRT_BATCH_SMALLEST_FIRST, pipelines: int = 0):
+                 max_wave_roots: int = 0, policy: int = capi.MRT_BATCH_SMALLEST_FIRST, pipelines: int = 0,
+                 kernel: int = 0):
         self.ctx = ctx
         self.lib = ctx.lib
         o = capi.MrtBatchOpts()
@@ -244,6 +245,7 @@ class Batch:
         o.max_wave_roots = max_wave_roots
         o.policy = policy
         o.pipelines = pipelines
+        o.kernel = kernel
         h = ctypes.c_void_p()
         ctx.check(self.lib.mrt_batch_create(ctx.h, ctypes.byref(o), ctypes.byref(h)), "mrt_batch_create")
         self.h = h

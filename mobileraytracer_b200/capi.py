@@ -24,6 +24,7 @@ MRT_PRIM_PLANE, MRT_PRIM_SPHERE, MRT_PRIM_TRIANGLE, MRT_PRIM_LIGHT = 0, 1, 2, 3
 MRT_HIT_NONE = 0xFFFFFFFF
 MRT_MEM_HOST, MRT_MEM_DEVICE = 0, 1
 MRT_BATCH_SMALLEST_FIRST, MRT_BATCH_FIFO, MRT_BATCH_EQUAL_SHARE = 0, 1, 2
+MRT_BATCH_KERNEL_WAVEFRONT, MRT_BATCH_KERNEL_PATHS = 1, 2
 RAY_LENGTH_MAX = 1.0e30
 
 STATUS_NAMES = {0: "MRT_OK", 1: "MRT_ERR_ARG", 2: "MRT_ERR_OOM", 3: "MRT_ERR_CUDA", 4: "MRT_ERR_LIMIT",
@@ -104,7 +105,7 @@ class MrtBatchOpts(ctypes.Structure):
     _fields_ = [("wave_roots", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
                 ("max_spl", ctypes.c_uint32), ("no_graph", ctypes.c_uint32), ("max_wave_roots", ctypes.c_uint32),
-                ("policy", ctypes.c_uint32), ("pipelines", ctypes.c_uint32)]
+                ("policy", ctypes.c_uint32), ("pipelines", ctypes.c_uint32), ("kernel", ctypes.c_uint32)]
 
 
 class MrtBatchJob(ctypes.Structure):
@@ -117,7 +118,7 @@ class MrtBatchStats(ctypes.Structure):
                 ("waves", ctypes.c_uint64), ("jobs_submitted", ctypes.c_uint64), ("jobs_done", ctypes.c_uint64),
                 ("busy_ms", ctypes.c_double), ("wave_roots", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("autotuned", ctypes.c_uint32), ("pipelines", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("kernel", ctypes.c_uint32), ("waves_paths", ctypes.c_uint64)]
 
 
 def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1, pixel_sampler=None,

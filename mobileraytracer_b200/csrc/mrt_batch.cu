@@ -25,7 +25,7 @@
 #include <vector>
 
 #include "mrt_internal.h"
-#include "mrt_wave.cuh"
+#include "mrt_paths.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
@@ -177,6 +177,61 @@ struct BatchShadowWork {
         }
     }
 };
+
+// whole camera paths in one persistent launch (mrt_paths.cuh): work item = the wave's path i
+struct BatchPathWork {
+    BatchState b;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return b.desc->n_roots; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ const DevScene &scene(const PathLane &L) const { return b.scenes[L.job]; }
+    __device__ const FastView &view(const PathLane &L) const { return L.v; }
+    __device__ const RenderParams &params(const PathLane &L) const { return b.jobs[L.job]; }
+    __device__ void begin(uint32_t i, PathLane &L, Ray &r) const {
+        const uint32_t n_seg = b.desc->n_seg;
+        uint32_t lo = 0, hi = n_seg;   // last segment with wave_off <= i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (b.desc->seg[mid].wave_off <= i) lo = mid; else hi = mid;
+        }
+        const Segment sg = b.desc->seg[lo];
+        const uint32_t local = sg.local_first + (i - sg.wave_off);
+        const RenderParams &p = b.jobs[sg.job];
+        Task k;
+        uint32_t pixel, sample;
+        path_of(p, local, k, pixel, sample);
+        L.st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+        r = primary_ray(p, k, L.st);
+        L.item = i;
+        L.job = sg.job;
+        L.v = fast_view(b.scenes[sg.job]);
+        L.top = 1;
+        L.fr[0].code = 1u;
+        L.fr[0].depth = 1;
+        L.fr[0].slot = 0;
+        b.root_job[i] = sg.job;
+        b.root_local[i] = local;
+    }
+    __device__ void deliver(const PathLane &L, V3 rgb, bool flag) const {
+        b.root_rgb[L.item] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
+    }
+    __device__ void count(uint32_t n_closest, uint32_t n_shadow) const {
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, n_closest), d = __reduce_add_sync(0xFFFFFFFFu, n_shadow);
+        if ((threadIdx.x & 31) == 0) {
+            if (!b.desc->dry) {
+                atomicAdd(&b.counters[0], (unsigned long long)c);
+                atomicAdd(&b.counters[1], (unsigned long long)d);
+            }
+            atomicAdd(&b.counters[2], (unsigned long long)c);
+            atomicAdd(&b.counters[3], (unsigned long long)d);
+        }
+    }
+};
+
+__global__ void __launch_bounds__(128, 8) k_batch_paths(BatchState b) {
+    BatchPathWork work{b, b.work};
+    persistent_paths(work);
+}
 
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_extend(BatchState b, int level) {
@@ -373,6 +428,7 @@ struct MrtBatch {
     cudaEvent_t ev_first = nullptr;  // start of the current busy period
     float period_ms = 0.0f;          // latest wave end seen in the current busy period
     uint64_t paths = 0;
+    uint64_t waves_paths = 0;        // waves run as whole-path launches
     double busy_ms = 0.0;
     unsigned long long counters_host[4] = {0, 0, 0, 0};
 };
@@ -408,11 +464,17 @@ void launch_traversal(const BatchState &s, int level, int grid, cudaStream_t q, 
 }
 
 // the wave up to the per-sample values: camera rays, every bounce level, the bottom-up resolve
+// (threads = 0: whole paths in one persistent launch instead)
 void launch_trace_kernels(MrtBatch *b, int pipe, uint32_t threads, uint32_t bps, cudaStream_t q) {
     const BatchState s = state_of(b, pipe);
     const int sm = b->ctx->sm_count;
     const int tgrid = sm * (int)bps;
     const int grid = sm * 16;
+    if (threads == 0) {
+        k_batch_begin<<<1, 64, 0, q>>>(s);
+        k_batch_paths<<<sm * 8, 128, 0, q>>>(s);
+        return;
+    }
     auto trav = [&](int level, bool extend) {
         if (threads == 64) launch_traversal<64>(s, level, tgrid, q, extend);
         else if (threads == 256) launch_traversal<256>(s, level, tgrid, q, extend);
@@ -456,20 +518,20 @@ int trace_graph(MrtBatch *b, int pipe, uint32_t threads, uint32_t bps, cudaGraph
 //   EQUAL_SHARE     an equal share for each of the first kMaxSegments jobs, leftovers to the
 //                   earliest (every job advances every wave; waves touch many scenes).
 // The first two fill a wave from as few jobs as possible, so the scenes a wave reads stay few.
-uint32_t plan_wave(MrtBatch *b, WaveDesc &d, uint32_t wave, bool commit, int64_t wave_index) {
+uint32_t plan_wave(MrtBatch *b, WaveDesc &d, uint32_t wave, bool commit, int64_t wave_index, uint32_t policy) {
     d.n_seg = 0;
     d.n_roots = 0;
     d.dry = commit ? 0u : 1u;
     if (b->active.empty()) return 0;
     std::vector<uint32_t> order(b->active);
-    if (b->opts.policy == MRT_BATCH_SMALLEST_FIRST)
+    if (policy == MRT_BATCH_SMALLEST_FIRST)
         std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
             return b->slots[x].total - b->slots[x].next < b->slots[y].total - b->slots[y].next;
         });
     const size_t n_act = std::min<size_t>(order.size(), kMaxSegments);
     std::vector<uint64_t> take(n_act, 0);
     uint64_t room = wave;
-    if (b->opts.policy == MRT_BATCH_EQUAL_SHARE) {
+    if (policy == MRT_BATCH_EQUAL_SHARE) {
         const uint64_t share = std::max<uint64_t>(1, wave / n_act);
         for (size_t a = 0; a < n_act && room; ++a) {
             const MrtBatch::Job &j = b->slots[order[a]];
@@ -507,6 +569,15 @@ uint32_t plan_wave(MrtBatch *b, WaveDesc &d, uint32_t wave, bool commit, int64_t
         b->active.swap(keep);
     }
     return off;
+}
+
+// Kernel of a wave when the caller left it open: whole paths per lane when no job holds half of
+// the wave (a mix of small jobs: level barriers and launches dominate the wavefront there), the
+// level-by-level wavefront when one job dominates (its rays are coherent level by level).
+bool whole_paths_wave(const WaveDesc &d) {
+    uint32_t largest = 0;
+    for (uint32_t k = 0; k < d.n_seg; ++k) largest = std::max(largest, d.seg[k].count);
+    return 2ull * largest < d.n_roots;
 }
 
 // one wave on pipeline `pipe`: description copy, the traced part (a graph replay), then the fold
@@ -591,7 +662,9 @@ int autotune(MrtBatch *b) {
     cudaStream_t q = ctx->stream;
     const MrtBatchOpts &o = b->opts;
     std::vector<std::pair<uint32_t, uint32_t>> shapes;
-    if (o.block_threads && o.blocks_per_sm) {
+    if (o.kernel == MRT_BATCH_KERNEL_PATHS) {
+        shapes.push_back({0u, 8u});
+    } else if (o.block_threads && o.blocks_per_sm) {
         shapes.push_back({o.block_threads, o.blocks_per_sm});
     } else {
         const uint32_t ts[3] = {64, 128, 256};
@@ -626,7 +699,8 @@ int autotune(MrtBatch *b) {
     auto probe = [&](uint32_t t, uint32_t bps, uint32_t w, uint32_t np, double &rate) -> int {
         WaveDesc &d = b->h_desc[0];
         rate = 0.0;
-        if (plan_wave(b, d, w, false, -1) == 0) return MRT_OK;
+        // an equal share of every queued job: the probe sees the batch's mix, not only its first jobs
+        if (plan_wave(b, d, w, false, -1, MRT_BATCH_EQUAL_SHARE) == 0) return MRT_OK;
         unsigned long long c0[4], c1[4];
         int st = read_counters(b, c0);
         if (st != MRT_OK) return st;
@@ -719,6 +793,14 @@ int mrt_batch_create(MrtContext *ctx, const MrtBatchOpts *opts, MrtBatch **out) 
     *out = nullptr;
     MrtBatchOpts o{};
     if (opts) o = *opts;
+    if (o.kernel == MRT_BATCH_KERNEL_PATHS && o.max_depth + 1 > (uint32_t)kPathFrames) {
+        set_error(ctx, "mrt_batch_create: whole-path launches hold depth_max <= %d", kPathFrames - 1);
+        return MRT_ERR_ARG;
+    }
+    if (o.kernel > MRT_BATCH_KERNEL_PATHS) {
+        set_error(ctx, "mrt_batch_create: kernel must be 0 (autotuned), MRT_BATCH_KERNEL_WAVEFRONT or MRT_BATCH_KERNEL_PATHS");
+        return MRT_ERR_ARG;
+    }
     if (o.block_threads && o.block_threads != 64 && o.block_threads != 128 && o.block_threads != 256) {
         set_error(ctx, "mrt_batch_create: block_threads must be 64, 128 or 256");
         return MRT_ERR_ARG;
@@ -891,11 +973,16 @@ int mrt_batch_step(MrtBatch *b, uint32_t max_waves, uint32_t *launched) {
         const int r = (int)(w % kRing);
         const int pipe = (int)(w % b->n_pipes);
         WaveDesc &d = b->h_desc[r];
-        const uint32_t n = plan_wave(b, d, b->wave_roots, true, w);
+        const uint32_t n = plan_wave(b, d, b->wave_roots, true, w, b->opts.policy);
         if (n == 0) break;
         if (b->waves_launched == b->waves_done) cudaEventRecord(b->ev_first, b->pipes[pipe].stream);
-        st = run_wave(b, d, pipe, b->block_threads, b->blocks_per_sm, r,
-                      w > b->waves_done ? (int)((w - 1) % kRing) : -1);
+        uint32_t threads = b->block_threads, bps = b->blocks_per_sm;
+        if (b->opts.kernel == 0 && b->n_levels <= kPathFrames && whole_paths_wave(d)) {
+            threads = 0;
+            bps = 8;
+            ++b->waves_paths;
+        }
+        st = run_wave(b, d, pipe, threads, bps, r, w > b->waves_done ? (int)((w - 1) % kRing) : -1);
         if (st != MRT_OK) return st;
         b->paths += n;
         ++b->waves_launched;
@@ -945,6 +1032,8 @@ int mrt_batch_stats(const MrtBatch *b, MrtBatchStats *out) {
     out->blocks_per_sm = b->blocks_per_sm;
     out->autotuned = b->autotuned;
     out->pipelines = b->n_pipes;
+    out->kernel = b->block_threads == 0 ? MRT_BATCH_KERNEL_PATHS : MRT_BATCH_KERNEL_WAVEFRONT;
+    out->waves_paths = b->block_threads == 0 ? (uint64_t)b->waves_launched : b->waves_paths;
     return MRT_OK;
 }
 

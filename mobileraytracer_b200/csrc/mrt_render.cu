@@ -23,7 +23,7 @@
 #include <mutex>
 
 #include "mrt_internal.h"
-#include "mrt_wave.cuh"
+#include "mrt_paths.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
@@ -290,6 +290,46 @@ __global__ void __launch_bounds__(128, 8) k_wave_shadow_fast(DevScene s, WaveSta
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[1], (unsigned long long)n);
 }
 
+// whole camera paths in one persistent launch (mrt_paths.cuh): work item = the wave's path i
+struct WavePathWork {
+    const DevScene *s;
+    const RenderParams *p;
+    WaveState w;
+    uint32_t *ctr;
+    __device__ uint32_t total() const { return w.n_roots; }
+    __device__ uint32_t *counter() const { return ctr; }
+    __device__ const DevScene &scene(const PathLane &) const { return *s; }
+    __device__ const DevScene &view(const PathLane &) const { return *s; }
+    __device__ const RenderParams &params(const PathLane &) const { return *p; }
+    __device__ void begin(uint32_t item, PathLane &L, Ray &r) const {
+        Task k;
+        uint32_t pixel, sample;
+        root_task(*p, w, item, k, pixel, sample);
+        L.st = make_stream(p->seed, pixel, sample, p->strata, p->constant_value);
+        r = primary_ray(*p, k, L.st);
+        L.item = item;
+        L.top = 1;
+        L.fr[0].code = 1u;
+        L.fr[0].depth = 1;
+        L.fr[0].slot = 0;
+    }
+    __device__ void deliver(const PathLane &L, V3 rgb, bool flag) const {
+        w.root_rgb[L.item] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
+    }
+    __device__ void count(uint32_t n_closest, uint32_t n_shadow) const {
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, n_closest), d = __reduce_add_sync(0xFFFFFFFFu, n_shadow);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&w.counters[0], (unsigned long long)c);
+            atomicAdd(&w.counters[1], (unsigned long long)d);
+        }
+    }
+};
+
+__global__ void __launch_bounds__(128, 8) k_wave_paths(DevScene s, RenderParams p, WaveState w, uint32_t *ctr) {
+    WavePathWork work{&s, &p, w, ctr};
+    persistent_paths(work);
+}
+
 // bottom-up evaluation of one level: the shade() bodies after their recursive calls return
 __global__ void __launch_bounds__(128) k_wave_resolve(DevScene s, RenderParams p, WaveState w, int level) {
     const Level L = clamp_level(w, w.levels[level]);
@@ -456,6 +496,18 @@ int cancelled(MrtContext *ctx, cudaStream_t q) {
     return MRT_ERR_CANCELLED;
 }
 
+// Renders of at most this many camera paths per pass run as whole-path launches, larger ones as the
+// level-by-level wavefront (MRT_PATHS_MAX; 0 = always the wavefront).  Measured on one B200: a
+// 256x256 Whitted frame 3.1x faster whole-path (launch-bound), a 512x512x4 PathTracer soup 1.2x
+// faster, a 1024x1024 terrain 1.1-1.3x slower (the wavefront's per-level coherence wins there).
+uint64_t paths_max_setting() {
+    static uint64_t v = [] {
+        const char *e = getenv("MRT_PATHS_MAX");
+        return e ? (uint64_t)atoll(e) : (uint64_t)(1u << 19);
+    }();
+    return v;
+}
+
 uint32_t wave_roots_setting() {
     static uint32_t v = [] {
         const char *e = getenv("MRT_WAVE_ROOTS");
@@ -548,17 +600,25 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         rays_closest = (uint64_t)plan.n_tasks * o->spp;
     } else {
         if (o->spl > 32) { set_error(ctx, "mrt_render: samplesLight above 32 is not supported by the wavefront"); return MRT_ERR_ARG; }
+        uint64_t all_roots = 0;
+        for (uint32_t c : plan.round_count) all_roots += (uint64_t)c * o->spp;
+        const bool paths = all_roots <= paths_max_setting() && accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST &&
+                           o->depth_max >= 0 && o->depth_max + 1 <= kPathFrames;
         uint64_t max_round = 0;
         for (uint32_t c : plan.round_count) max_round = std::max<uint64_t>(max_round, c);
-        const uint32_t wave = (uint32_t)std::min<uint64_t>(max_round * o->spp, wave_roots_setting());
+        const uint32_t wave = (uint32_t)std::min<uint64_t>(max_round * o->spp,
+                                                           paths ? std::max(wave_roots_setting(), 1u << 22)
+                                                                 : wave_roots_setting());
         const int levels = std::max(1, o->depth_max + 1);
-        const uint64_t ray_cap = (uint64_t)wave * (uint64_t)(levels + 2);
-        const uint64_t shadow_cap = (uint64_t)wave * std::max(1u, o->spl) * 2ull;
+        const uint64_t ray_cap = paths ? 0 : (uint64_t)wave * (uint64_t)(levels + 2);
+        const uint64_t shadow_cap = paths ? 0 : (uint64_t)wave * std::max(1u, o->spl) * 2ull;
         if (ray_cap > 0xFFFFFFF0ull) { set_error(ctx, "mrt_render: wave too large"); return MRT_ERR_ARG; }
         if (2 * (levels + 1) > 64) { set_error(ctx, "mrt_render: depth_max above 30"); return MRT_ERR_ARG; }
-        if (st == MRT_OK) st = ensure(ctx, ctx->wave[1], sizeof(RayRec) * ray_cap);
-        if (st == MRT_OK) st = ensure(ctx, ctx->wave[2], sizeof(NodeRec) * ray_cap);
-        if (st == MRT_OK) st = ensure(ctx, ctx->wave[3], sizeof(ShadowRec) * shadow_cap);
+        if (!paths) {   // the wavefront's queues (whole-path launches keep their state per lane)
+            if (st == MRT_OK) st = ensure(ctx, ctx->wave[1], sizeof(RayRec) * ray_cap);
+            if (st == MRT_OK) st = ensure(ctx, ctx->wave[2], sizeof(NodeRec) * ray_cap);
+            if (st == MRT_OK) st = ensure(ctx, ctx->wave[3], sizeof(ShadowRec) * shadow_cap);
+        }
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[4], sizeof(Level) * (levels + 2));
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[5], sizeof(float4) * wave);
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[6], 16);
@@ -590,12 +650,17 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 if (s->stop.load()) return cancelled(ctx, q);
                 w.root_first = (uint32_t)r0;
                 w.n_roots = (uint32_t)std::min<uint64_t>(wave, total_roots - r0);
-                cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
-                cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
-                k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
-                for (int b = 0; b < levels; ++b)
-                    MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);
-                for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
+                if (paths) {
+                    cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
+                    k_wave_paths<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, w, ctx->d_counters);
+                } else {
+                    cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
+                    cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
+                    k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
+                    for (int b = 0; b < levels; ++b)
+                        MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);
+                    for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
+                }
                 k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
                 const int slot = (int)(waves_issued % 2);
                 cudaEventRecord(ctx->wave_ev[slot], q);

@@ -93,6 +93,9 @@ def plain_and_batched(ctx, batch_kwargs, repeat_jobs=1):
     dict(wave_roots=7777, policy=capi.MRT_BATCH_EQUAL_SHARE, pipelines=3),  # every job in every wave
     dict(wave_roots=2000, pipelines=4, block_threads=256, blocks_per_sm=4),  # 4 waves in flight
     dict(max_wave_roots=1 << 16),                                            # autotuned
+    dict(wave_roots=3001, kernel=capi.MRT_BATCH_KERNEL_PATHS, pipelines=2),   # whole paths per lane
+    dict(wave_roots=50000, kernel=capi.MRT_BATCH_KERNEL_PATHS, pipelines=4,
+         policy=capi.MRT_BATCH_EQUAL_SHARE),
 ])
 def test_batch_equals_plain(ctx, kw):
     plain, batched, ids, done, stats, rays = plain_and_batched(ctx, kw)
@@ -107,11 +110,13 @@ def test_batch_equals_plain(ctx, kw):
     assert stats.paths == sum(o.width * o.height * o.spp for _, _, o, _, _ in job_list())
     if kw.get("wave_roots") == 3001:
         assert stats.waves >= stats.paths // 3001
-        assert stats.wave_roots == 3001 and stats.autotuned == 0
+        assert stats.wave_roots == 3001 and (stats.autotuned == 0 or "kernel" in kw)
     if "max_wave_roots" in kw:
         assert stats.autotuned > 1 and stats.block_threads in (64, 128, 256) and 1 <= stats.pipelines <= 4
     if "pipelines" in kw:
         assert stats.pipelines == kw["pipelines"]
+    if "kernel" in kw:
+        assert stats.kernel == kw["kernel"]
 
 
 def test_batch_many_jobs_share_waves(ctx):

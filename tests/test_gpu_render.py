@@ -6,6 +6,8 @@ NoShadows, Whitted and PathTracer frames must equal the oracle bit for bit: the 
 specification allows (1e-4 for the deterministic shaders, 1e-3 for PathTracer radiance) is asserted
 on the fp32 sums as the documented bound; the bitmaps are compared exactly.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -200,3 +202,37 @@ def test_stop_and_progress(ctx):
     assert 0 < seen < 512
     small = capi.render_opts(shader=PT, width=64, height=64, spp=2, spl=1)
     g.render(sc.camera, small)   # no error: the stop request was consumed
+
+
+def test_whole_paths_equal_wavefront(ctx, tmp_path):
+    """The same PathTracer and Whitted frames from whole-path launches (small frames, this process)
+    and from the level-by-level wavefront (a process with MRT_PATHS_MAX=0)."""
+    import subprocess
+    import sys
+    code = (
+        "import sys, numpy as np\n"
+        "sys.path.insert(0, %r)\n"
+        "import mobileraytracer_b200 as m\n"
+        "from mobileraytracer_b200 import capi, scenes\n"
+        "ctx = m.Context(0)\n"
+        "out = []\n"
+        "for sh in (1, 2):\n"
+        "    sc = scenes.glass_room()\n"
+        "    o = capi.render_opts(shader=sh, width=96, height=64, spp=3, spl=2, seed=7)\n"
+        "    g = m.Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)\n"
+        "    bm, acc, st = g.render(sc.camera, o, accum=np.zeros((64, 96, 4), np.float32))\n"
+        "    out += [bm, acc, np.array([st.rays_closest, st.rays_shadow], np.uint64)]\n"
+        "np.savez(sys.argv[1], *out)\n" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),))
+    path = str(tmp_path / "wf.npz")
+    env = dict(os.environ, MRT_PATHS_MAX="0")
+    r = subprocess.run([sys.executable, "-c", code, path], env=env, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    wf = np.load(path)
+    for k, sh in enumerate((WH, PT)):
+        sc = scenes.glass_room()
+        o = capi.render_opts(shader=sh, width=96, height=64, spp=3, spl=2, seed=7)
+        g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
+        bm, acc, st = g.render(sc.camera, o, accum=np.zeros((64, 96, 4), np.float32))
+        assert np.array_equal(bm, wf[f"arr_{3 * k}"])
+        assert np.array_equal(acc.view(np.uint32), wf[f"arr_{3 * k + 1}"].view(np.uint32))
+        assert [st.rays_closest, st.rays_shadow] == list(wf[f"arr_{3 * k + 2}"])
