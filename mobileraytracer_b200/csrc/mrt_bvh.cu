@@ -448,7 +448,7 @@ namespace mrt_host {
 int leaf_max_setting() {
     static int v = [] {
         const char *e = getenv("MRT_BVH_LEAF_MAX");
-        const int x = e ? atoi(e) : 4;
+        const int x = e ? atoi(e) : 3;   // 3: fastest of 2..8 on the soup frame and a PathTracer job
         return x < 1 ? 1 : (x > 16 ? 16 : x);
     }();
     return v;
