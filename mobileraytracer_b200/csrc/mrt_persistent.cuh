@@ -25,6 +25,7 @@ struct FastTrav {
     uint32_t best_i;
     uint32_t node;          // node to expand next (kNodeNone: pop the stack)
     uint32_t leaf_first, leaf_count;   // pending leaf (count 0: none)
+    uint32_t leaf2_first, leaf2_count; // a second leaf found while waiting for the warp (speculative)
     int sp;
     bool have;
     uint32_t c_nodes, c_tris;
@@ -44,6 +45,7 @@ __device__ __forceinline__ void trav_begin(const DevScene &s, const Ray &r, floa
     t.have = false;
     t.node = s.n_tri == 0 ? kNodeNone : 0u;   // the root node
     t.leaf_count = 0;
+    t.leaf2_count = 0;
     t.sp = 0;
     t.c_nodes = 0;
     t.c_tris = 0;
@@ -52,14 +54,25 @@ __device__ __forceinline__ void trav_begin(const DevScene &s, const Ray &r, floa
 __device__ __forceinline__ bool trav_wants_node(const FastTrav &t) {
     return t.leaf_count == 0 && (t.node != kNodeNone || t.sp > 0);
 }
+// a lane with one pending leaf may go on with node steps while others of its warp still search
+// (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs", HPG 2009: speculative
+// traversal), up to a second leaf
+__device__ __forceinline__ bool trav_can_speculate(const FastTrav &t) {
+    return t.leaf_count > 0 && t.leaf2_count == 0 && (t.node != kNodeNone || t.sp > 0);
+}
 __device__ __forceinline__ bool trav_finished(const FastTrav &t) {
-    return t.leaf_count == 0 && t.node == kNodeNone && t.sp == 0;
+    return t.leaf_count == 0 && t.leaf2_count == 0 && t.node == kNodeNone && t.sp == 0;
 }
 
 __device__ __forceinline__ void trav_take(FastTrav &t, uint32_t code) {
     if (code & kLeafCode) {
-        t.leaf_first = code_first(code);
-        t.leaf_count = code_count(code);
+        if (t.leaf_count == 0) {
+            t.leaf_first = code_first(code);
+            t.leaf_count = code_count(code);
+        } else {
+            t.leaf2_first = code_first(code);
+            t.leaf2_count = code_count(code);
+        }
         t.node = kNodeNone;
     } else {
         t.node = code;
@@ -95,8 +108,10 @@ template <bool kCount, class S>
 __device__ __forceinline__ void trav_leaf_step(const S &s, const Ray &r, FastTrav &t) {
     FastCounts cnt{0, 0};
     fast_leaf<kCount>(s, r, t.leaf_first, t.leaf_count, t.best_t, t.best_i, t.have, cnt);
+    if (t.leaf2_count) fast_leaf<kCount>(s, r, t.leaf2_first, t.leaf2_count, t.best_t, t.best_i, t.have, cnt);
     if (kCount) t.c_tris += cnt.tris;
     t.leaf_count = 0;
+    t.leaf2_count = 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -154,11 +169,11 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             if (exhausted) break;
             continue;
         }
-        // 2. node phase
+        // 2. node phase (lanes holding a leaf step on speculatively while others search)
         for (;;) {
             const bool w = active && trav_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) trav_node_step<kCount>(work.view(lane, s), t, stk);
+            if (w || (active && trav_can_speculate(t))) trav_node_step<kCount>(work.view(lane, s), t, stk);
         }
         // 3. leaf phase
         if (active && t.leaf_count > 0) trav_leaf_step<kCount>(work.view(lane, s), r, t);
