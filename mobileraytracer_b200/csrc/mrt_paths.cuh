@@ -163,21 +163,25 @@ __device__ __forceinline__ bool path_next(const DevScene &s, const RenderParams 
 // first occluder ends the query), Shader::shadowTrace (Shader.cpp:162-187)
 template <class S>
 __device__ __forceinline__ void occ_leaf_on_trav(const S &s, const Ray &r, FastTrav &t) {
-    const uint32_t first = t.leaf_first, count = t.leaf_count;
-    t.leaf_count = 0;
-    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
-    for (uint32_t k = first; k < first + count; ++k) {
-        const float4 A = __ldg(&s.ftris[3 * k]);
-        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
-        if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
-        if (tri_occ(v3(A), v3(AB), v3(AC), r, t.best_t)) {
-            t.have = true;
-            t.node = kNodeNone;
-            t.sp = 0;
-            return;
+    for (int q = 0; q < 2; ++q) {
+        const uint32_t first = q == 0 ? t.leaf_first : t.leaf2_first, count = q == 0 ? t.leaf_count : t.leaf2_count;
+        if (count == 0) continue;
+        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4 A = __ldg(&s.ftris[3 * k]);
+            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
+            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
+            if (tri_occ(v3(A), v3(AB), v3(AC), r, t.best_t)) {
+                t.have = true;
+                t.node = kNodeNone;
+                t.sp = 0;
+                t.leaf_count = t.leaf2_count = 0;
+                return;
+            }
         }
     }
+    t.leaf_count = t.leaf2_count = 0;
 }
 
 // Work provides: total(), counter(), scene(lane), view(lane), params(lane),
@@ -242,10 +246,10 @@ __device__ void persistent_paths(Work &work) {
             continue;
         }
         // 2. node phase
-        for (;;) {
+        for (;;) {   // lanes holding a leaf step on speculatively while others search
             const bool w = active && trav_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) trav_node_step<false>(work.view(lane), t, stk);
+            if (w || (active && trav_can_speculate(t))) trav_node_step<false>(work.view(lane), t, stk);
         }
         // 3. leaf phase
         if (active && t.leaf_count > 0) {

@@ -204,6 +204,7 @@ struct OccTrav {
     float dist;
     uint32_t node;
     uint32_t leaf_first, leaf_count;
+    uint32_t leaf2_first, leaf2_count;   // speculative second leaf
     int sp;
     bool occluded;
 };
@@ -212,6 +213,7 @@ __device__ __forceinline__ void occ_begin(const DevScene &s, const Ray &r, float
     t.dist = dist;
     t.node = kNodeNone;
     t.leaf_count = 0;
+    t.leaf2_count = 0;
     t.sp = 0;
     t.occluded = naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist);
     if (t.occluded || s.n_tri == 0) return;
@@ -222,14 +224,22 @@ __device__ __forceinline__ void occ_begin(const DevScene &s, const Ray &r, float
 __device__ __forceinline__ bool occ_wants_node(const OccTrav &t) {
     return !t.occluded && t.leaf_count == 0 && (t.node != kNodeNone || t.sp > 0);
 }
+__device__ __forceinline__ bool occ_can_speculate(const OccTrav &t) {
+    return !t.occluded && t.leaf_count > 0 && t.leaf2_count == 0 && (t.node != kNodeNone || t.sp > 0);
+}
 __device__ __forceinline__ bool occ_finished(const OccTrav &t) {
-    return t.occluded || (t.leaf_count == 0 && t.node == kNodeNone && t.sp == 0);
+    return t.occluded || (t.leaf_count == 0 && t.leaf2_count == 0 && t.node == kNodeNone && t.sp == 0);
 }
 
 __device__ __forceinline__ void occ_take(OccTrav &t, uint32_t code) {
     if (code & kLeafCode) {
-        t.leaf_first = code_first(code);
-        t.leaf_count = code_count(code);
+        if (t.leaf_count == 0) {
+            t.leaf_first = code_first(code);
+            t.leaf_count = code_count(code);
+        } else {
+            t.leaf2_first = code_first(code);
+            t.leaf2_count = code_count(code);
+        }
         t.node = kNodeNone;
     } else {
         t.node = code;
@@ -257,16 +267,20 @@ __device__ __forceinline__ void occ_node_step(const S &s, OccTrav &t, uint32_t *
 
 template <class S>
 __device__ __forceinline__ void occ_leaf_step(const S &s, const Ray &r, OccTrav &t) {
-    const uint32_t first = t.leaf_first, count = t.leaf_count;
-    t.leaf_count = 0;
-    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
-    for (uint32_t k = first; k < first + count; ++k) {
-        const float4 A = __ldg(&s.ftris[3 * k]);
-        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
-        if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
-        if (tri_occ(v3(A), v3(AB), v3(AC), r, t.dist)) { t.occluded = true; return; }
+    for (int q = 0; q < 2 && !t.occluded; ++q) {
+        const uint32_t first = q == 0 ? t.leaf_first : t.leaf2_first, count = q == 0 ? t.leaf_count : t.leaf2_count;
+        if (count == 0) continue;
+        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4 A = __ldg(&s.ftris[3 * k]);
+            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
+            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
+            if (tri_occ(v3(A), v3(AB), v3(AC), r, t.dist)) { t.occluded = true; break; }
+        }
     }
+    t.leaf_count = 0;
+    t.leaf2_count = 0;
 }
 
 template <class Work, class Lane>
@@ -303,7 +317,7 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
         for (;;) {
             const bool w = active && occ_wants_node(t);
             if (!__any_sync(FULL, w)) break;
-            if (w) occ_node_step(work.view(lane, s), t, stack_n);
+            if (w || (active && occ_can_speculate(t))) occ_node_step(work.view(lane, s), t, stack_n);
         }
         if (active && t.leaf_count > 0) occ_leaf_step(work.view(lane, s), r, t);
         if (active && occ_finished(t)) {
