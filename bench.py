@@ -494,9 +494,9 @@ def bench_scene(args):
     clocks.__exit__(None, None, None)
     value = rays / (dev_ms / 1e3) / 1e6
     rays_per_path = rays / paths
-    # end to end: host bitmap and sums in and out through the C ABI
-    host_bm = np.zeros((h, w), np.uint32)
-    host_acc = np.zeros((h, w, 4), np.float32)
+    # end to end: host bitmap and sums (pinned) in and out through the C ABI
+    host_bm = torch.zeros((h, w), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    host_acc = torch.zeros((h, w, 4), dtype=torch.float32).pin_memory().numpy()
     scene.render(sc.camera, opts, bitmap=host_bm, accum=host_acc)
     n_e2e = max(1, min(args.e2e_steps, args.steps))
     t1 = time.perf_counter()
