@@ -31,10 +31,13 @@ struct FastTrav {
     uint32_t c_nodes, c_tris;
 };
 
-// the traversal stack lives apart from the scalar state so the scalars stay in registers
+// the traversal stack lives apart from the scalar state so the scalars stay in registers.  It holds
+// node and leaf codes only: a popped entry is not culled by its entry distance (the children of a
+// popped node still meet the box test against the best distance).  Keeping the distances and
+// culling at the pop cost one more local load and store per entry and was 8 % slower on the
+// 1,000,000-triangle soup frame than expanding the few entries it would have culled.
 struct TravStack {
     uint32_t n[kFastStack];
-    float t[kFastStack];
 };
 
 template <bool kCount>
@@ -79,15 +82,12 @@ __device__ __forceinline__ void trav_take(FastTrav &t, uint32_t code) {
     }
 }
 
-// one node step: expand the current node (popping one first, with distance culling, when there is
-// none), nearest child next and the other hits pushed far to near
+// one node step: expand the current node (popping one first when there is none), nearest child
+// next and the other hits pushed far to near
 template <bool kCount, class S>
 __device__ __forceinline__ void trav_node_step(const S &s, FastTrav &t, TravStack &st) {
     if (t.node == kNodeNone) {
-        while (t.sp > 0) {
-            --t.sp;
-            if (st.t[t.sp] <= t.best_t * 1.000001f) { trav_take(t, st.n[t.sp]); break; }
-        }
+        if (t.sp > 0) { --t.sp; trav_take(t, st.n[t.sp]); }
         if (t.node == kNodeNone) return;   // a leaf, or nothing left
     }
     if (!node_in_range(s, t.node)) { raise_error(s, MRT_ERR_LIMIT); t.node = kNodeNone; t.sp = 0; return; }
@@ -100,7 +100,7 @@ __device__ __forceinline__ void trav_node_step(const S &s, FastTrav &t, TravStac
     if (t.sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); t.sp = 0; return; }
 #pragma unroll
     for (int k = kWide - 1; k >= 1; --k)
-        if (k < n) { st.n[t.sp] = cc[k]; st.t[t.sp] = ct[k]; ++t.sp; }
+        if (k < n) { st.n[t.sp] = cc[k]; ++t.sp; }
     trav_take(t, cc[0]);
 }
 
