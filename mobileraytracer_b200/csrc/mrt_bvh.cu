@@ -7,7 +7,7 @@
 // FAST tree: built on the device.  Triangle boxes padded outward -> 30-bit Morton codes of the
 // centroids -> stable LSD radix sort (own kernels) -> Karras' parallel hierarchy ("Maximizing
 // parallelism in the construction of BVHs, octrees and k-d trees", HPG 2012) -> bottom-up box fit
-// -> records in child-pair layout (32 bytes per record), subtrees of <= kLeafMax triangles collapsed
+// -> records in child-pair layout (32 bytes per record), subtrees of <= leaf_max_setting() triangles collapsed
 // into leaves -> the binary tree collapsed into kWide-wide nodes (one 128-byte node = the kWide
 // child records a traversal step tests; each wide node opens the largest internal children of a
 // binary node until it is full), wide nodes numbered level by level -> triangles copied in leaf
@@ -448,7 +448,7 @@ namespace mrt_host {
 int leaf_max_setting() {
     static int v = [] {
         const char *e = getenv("MRT_BVH_LEAF_MAX");
-        const int x = e ? atoi(e) : 3;   // 3: fastest of 2..8 on the soup frame and a PathTracer job
+        const int x = e ? atoi(e) : 2;   // 2: fastest of 2..4 on the soup frame, a PathTracer job and the batch
         return x < 1 ? 1 : (x > 16 ? 16 : x);
     }();
     return v;

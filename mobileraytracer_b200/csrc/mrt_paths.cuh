@@ -248,7 +248,7 @@ __device__ void persistent_paths(Work &work) {
         // 2. node phase
         for (;;) {   // lanes holding a leaf step on speculatively while others search
             const bool w = active && trav_wants_node(t);
-            if (!__any_sync(FULL, w)) break;
+            if (node_phase_over(w, active && t.leaf_count > 0)) break;
             if (w || (active && trav_can_speculate(t))) trav_node_step<false>(work.view(lane), t, stk);
         }
         // 3. leaf phase

@@ -67,6 +67,15 @@ __device__ __forceinline__ bool trav_finished(const FastTrav &t) {
     return t.leaf_count == 0 && t.leaf2_count == 0 && t.node == kNodeNone && t.sp == 0;
 }
 
+// the node phase of a warp ends when no lane searches any more, or when fewer than kNodeQuorum lanes
+// search while others hold leaves: those leaves are tested first, and the few searching lanes go on
+// in the next node phase (2 and 4: +2 % on the 1,000,000-triangle soup frame, 8: -2 %)
+constexpr int kNodeQuorum = 4;
+__device__ __forceinline__ bool node_phase_over(bool searching, bool holding_leaf) {
+    const uint32_t s = __ballot_sync(0xFFFFFFFFu, searching);
+    return s == 0u || (__popc(s) < kNodeQuorum && __any_sync(0xFFFFFFFFu, holding_leaf));
+}
+
 __device__ __forceinline__ void trav_take(FastTrav &t, uint32_t code) {
     if (code & kLeafCode) {
         if (t.leaf_count == 0) {
@@ -172,7 +181,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
         // 2. node phase (lanes holding a leaf step on speculatively while others search)
         for (;;) {
             const bool w = active && trav_wants_node(t);
-            if (!__any_sync(FULL, w)) break;
+            if (node_phase_over(w, active && t.leaf_count > 0)) break;
             if (w || (active && trav_can_speculate(t))) trav_node_step<kCount>(work.view(lane, s), t, stk);
         }
         // 3. leaf phase
@@ -316,7 +325,7 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
         }
         for (;;) {
             const bool w = active && occ_wants_node(t);
-            if (!__any_sync(FULL, w)) break;
+            if (node_phase_over(w, active && t.leaf_count > 0)) break;
             if (w || (active && occ_can_speculate(t))) occ_node_step(work.view(lane, s), t, stack_n);
         }
         if (active && t.leaf_count > 0) occ_leaf_step(work.view(lane, s), r, t);
