@@ -7,11 +7,11 @@
 // FAST tree: built on the device.  Triangle boxes padded outward -> 30-bit Morton codes of the
 // centroids -> stable LSD radix sort (own kernels) -> Karras' parallel hierarchy ("Maximizing
 // parallelism in the construction of BVHs, octrees and k-d trees", HPG 2012) -> bottom-up box fit
-// -> records in child-pair layout (32 bytes per record), subtrees of <= leaf_max_setting() triangles collapsed
-// into leaves -> the binary tree collapsed into kWide-wide nodes (one 128-byte node = the kWide
-// child records a traversal step tests; each wide node opens the largest internal children of a
-// binary node until it is full), wide nodes numbered level by level -> triangles copied in leaf
-// order as 48-byte records.  A traversal step of the wide tree replaces about two of the binary
+// -> records in child-pair layout (32 bytes per record), subtrees of <= leaf_max_setting()
+// triangles collapsed into leaves where the surface-area cost says so -> the binary tree collapsed
+// into kWide-wide nodes (one 128-byte node = the kWide child records a traversal step tests; each
+// wide node opens the largest internal children of a binary node until it is full), wide nodes
+// numbered level by level -> triangles copied in leaf order as 48-byte records.  A traversal step of the wide tree replaces about two of the binary
 // tree's, halving the chain of dependent node fetches per ray.
 #include <algorithm>
 #include <cstdlib>
@@ -320,6 +320,72 @@ __device__ __forceinline__ void write_record(float4 *rec, float4 lo, float4 hi, 
     rec[1] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(b));
 }
 
+__device__ __forceinline__ float half_area(float4 lo, float4 hi) {
+    const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// --- leaf choice -------------------------------------------------------------------------------
+// A subtree of at most leaf_max triangles becomes one leaf when that is cheaper by the surface-area
+// cost model than keeping its inner nodes.  Per ray that reaches the subtree's box, a leaf costs
+// kTriCost per triangle; an inner node costs kNodeCost plus its two children's costs, each weighted
+// by the share of the node's box area its box has.  The unit is one box test: 2.2 box tests per
+// triangle test and 2 per opened inner node fit the frame times of the 1,000,000-triangle soup at
+// leaves of 1, 2 and 3 triangles.  Scattered small triangles (the soups) end up one per leaf: two
+// boxes cull better than two triangle tests; touching triangles (a heightfield) stay in pairs.
+constexpr float kTriCost = 2.2f, kNodeCost = 2.0f;
+constexpr int kLeafCostDepth = 3;   // inner levels of a subtree of up to 4 triangles
+
+struct BinView {
+    const uint32_t *vals;
+    const float4 *bmin, *bmax;
+    const uint32_t *left, *right, *first, *last;
+    const float4 *imin, *imax;
+    __device__ void box(uint32_t c, float4 &lo, float4 &hi) const {
+        if (c & kLeafBit) {
+            const uint32_t t = vals[c & ~kLeafBit];
+            lo = bmin[t];
+            hi = bmax[t];
+        } else {
+            lo = imin[c];
+            hi = imax[c];
+        }
+    }
+    __device__ uint32_t count(uint32_t c) const { return (c & kLeafBit) ? 1u : last[c] - first[c] + 1u; }
+};
+
+template <int D>
+__device__ float subtree_cost(const BinView &v, uint32_t c);
+
+template <int D>
+__device__ float split_cost(const BinView &v, uint32_t c) {
+    float4 lo, hi;
+    v.box(c, lo, hi);
+    const float a = half_area(lo, hi);
+    float cost = kNodeCost;
+    const uint32_t ch[2] = {v.left[c], v.right[c]};
+    for (int k = 0; k < 2; ++k) {
+        float4 l2, h2;
+        v.box(ch[k], l2, h2);
+        const float share = a > 0.0f ? half_area(l2, h2) / a : 1.0f;
+        cost += share * subtree_cost<D - 1>(v, ch[k]);
+    }
+    return cost;
+}
+
+template <int D>
+__device__ float subtree_cost(const BinView &v, uint32_t c) {
+    if (c & kLeafBit) return kTriCost;
+    const float leaf = kTriCost * (float)v.count(c);
+    if constexpr (D == 0) return leaf;
+    else return fminf(leaf, split_cost<D>(v, c));
+}
+
+// inner node c (count <= leaf_max) as one leaf?
+__device__ __forceinline__ bool leaf_by_cost(const BinView &v, uint32_t c) {
+    return kTriCost * (float)v.count(c) <= split_cost<kLeafCostDepth>(v, c);
+}
+
 // one record per child of every internal node (pair at 2 + 2k), plus the root record 0
 __global__ void k_emit(int n, int leaf_max, const uint32_t *__restrict__ vals, const float4 *__restrict__ bmin,
                        const float4 *__restrict__ bmax, const uint32_t *__restrict__ left, const uint32_t *__restrict__ right,
@@ -327,9 +393,10 @@ __global__ void k_emit(int n, int leaf_max, const uint32_t *__restrict__ vals, c
                        const float4 *__restrict__ imax, float4 *records) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n - 1) return;
+    const BinView v{vals, bmin, bmax, left, right, first, last, imin, imax};
     if (k == 0) {
         const uint32_t cnt = last[0] - first[0] + 1;
-        if ((int)cnt <= leaf_max) write_record(records, imin[0], imax[0], first[0], cnt);
+        if ((int)cnt <= leaf_max && leaf_by_cost(v, 0u)) write_record(records, imin[0], imax[0], first[0], cnt);
         else write_record(records, imin[0], imax[0], 2u, 0u);
         write_record(records + 2, make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), 0u, 0u);
     }
@@ -346,7 +413,7 @@ __global__ void k_emit(int n, int leaf_max, const uint32_t *__restrict__ vals, c
             lo = imin[c];
             hi = imax[c];
             const uint32_t cnt = last[c] - first[c] + 1;
-            if ((int)cnt <= leaf_max) write_record(rec, lo, hi, first[c], cnt);
+            if ((int)cnt <= leaf_max && leaf_by_cost(v, c)) write_record(rec, lo, hi, first[c], cnt);
             else write_record(rec, lo, hi, 2u + 2u * c, 0u);
         }
     }
@@ -372,11 +439,6 @@ struct CollapseItem {
     uint32_t bin;    // binary internal node (children at records 2 + 2 bin, 3 + 2 bin)
     uint32_t wide;   // wide node it becomes
 };
-
-__device__ __forceinline__ float half_area(float4 lo, float4 hi) {
-    const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
-    return dx * dy + dy * dz + dz * dx;
-}
 
 __device__ __forceinline__ void write_empty_slot(float4 *rec) {
     rec[0] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
@@ -448,7 +510,7 @@ namespace mrt_host {
 int leaf_max_setting() {
     static int v = [] {
         const char *e = getenv("MRT_BVH_LEAF_MAX");
-        const int x = e ? atoi(e) : 2;   // 2: fastest of 2..4 on the soup frame, a PathTracer job and the batch
+        const int x = e ? atoi(e) : 4;   // the largest subtree the surface-area leaf choice may keep as one leaf
         return x < 1 ? 1 : (x > 16 ? 16 : x);
     }();
     return v;
