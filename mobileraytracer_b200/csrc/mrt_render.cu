@@ -60,15 +60,13 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
 }
 
 // persistent FAST-BVH NoShadows: work item = pixel task; the lane traces the pixel's samples in
-// order and keeps its running mean in registers.  Implicit tasks are fetched in 8x4-pixel tiles
-// (when the image allows) so the rays of a warp start coherent.
+// order.  Only the task number and the sample count stay in registers while a ray is traced: the
+// pixel's running mean and fp32 sums are read and written back at the end of each sample (a few
+// bytes per ray), which leaves the registers to the traversal.  Implicit tasks are fetched in
+// 8x4-pixel tiles (when the image allows) so the rays of a warp start coherent.
 struct NsLane {
-    Task k;
-    uint32_t pixel;
-    int64_t slot;
-    uint32_t bm;
-    float4 acc;
-    uint32_t si;
+    uint32_t t;    // task number
+    uint32_t si;   // samples done
 };
 
 struct NsWork {
@@ -84,8 +82,9 @@ struct NsWork {
     template <class L>
     __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
     __device__ Ray ray_for(const NsLane &lane) const {
-        const Stream st = make_stream(p->seed, lane.pixel, p->spp_offset + lane.si, p->strata, p->constant_value);
-        return primary_ray(*p, lane.k, st);
+        const Task k = task_of(*p, lane.t);
+        const Stream st = make_stream(p->seed, k.y * p->width + k.x, p->spp_offset + lane.si, p->strata, p->constant_value);
+        return primary_ray(*p, k, st);
     }
     __device__ bool begin(uint32_t item, NsLane &lane, Ray &r) const {
         uint32_t t = first + item;
@@ -94,33 +93,33 @@ struct NsWork {
             const uint32_t x = (tile % tiles_x) * 8u + (w & 7u), y = (tile / tiles_x) * 4u + (w >> 3);
             t = y * p->width + x;
         }
-        lane.k = task_of(*p, t);
-        lane.pixel = lane.k.y * p->width + lane.k.x;
-        lane.slot = p->accum ? accum_slot(*p, lane.k) : -1;
-        lane.bm = p->bitmap[lane.k.index];
-        lane.acc = lane.slot >= 0 ? p->accum[lane.slot] : make_float4(0, 0, 0, 0);
+        lane.t = t;
         lane.si = 0;
         r = ray_for(lane);
         return true;
     }
     __device__ bool finish(NsLane &lane, Ray &r, bool hit, float, uint32_t id, const FastTrav &) const {
+        const Task k = task_of(*p, lane.t);
         const uint32_t sample = p->spp_offset + lane.si;
         V3 rgb{0.0f, 0.0f, 0.0f};
         if (hit) {
             Isect it;
             if (make_isect(*s, r, id, it)) {
-                const Stream st = make_stream(p->seed, lane.pixel, sample, p->strata, p->constant_value);
+                const Stream st = make_stream(p->seed, k.y * p->width + k.x, sample, p->strata, p->constant_value);
                 rgb = shade_direct(*s, *p, st, r, it);
             }
         }
-        lane.bm = incremental_avg(rgb, lane.bm, sample + 1u);
-        lane.acc.x += rgb.x; lane.acc.y += rgb.y; lane.acc.z += rgb.z; lane.acc.w += 1.0f;
+        p->bitmap[k.index] = incremental_avg(rgb, p->bitmap[k.index], sample + 1u);
+        const int64_t slot = p->accum ? accum_slot(*p, k) : -1;
+        if (slot >= 0) {
+            float4 acc = p->accum[slot];
+            acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
+            p->accum[slot] = acc;
+        }
         if (++lane.si < p->spp) {
             r = ray_for(lane);
             return true;
         }
-        p->bitmap[lane.k.index] = lane.bm;
-        if (lane.slot >= 0) p->accum[lane.slot] = lane.acc;
         return false;
     }
 };
