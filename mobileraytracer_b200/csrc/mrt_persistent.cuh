@@ -6,8 +6,9 @@
 // resumable traversal state and the warp loops:
 //   1. refill: lanes whose work item is finished take new items from a global counter, one
 //      atomicAdd per warp for all of them (ballot + popc);
-//   2. node phase: lanes that have no pending leaf visit node pairs until every lane has found a
-//      leaf or finished (warp vote), so node visits of different lanes run together;
+//   2. node phase: lanes that have no pending leaf expand 4-wide nodes until fewer than
+//      kNodeQuorum lanes still search (warp vote), so node visits of different lanes run
+//      together; lanes holding one leaf go on speculatively up to a second one;
 //   3. leaf phase: pending leaves are intersected together;
 //   4. completion: finished rays hand their result to the work item, which may start its next
 //      ray in the same lane (e.g. the next sample of a pixel).

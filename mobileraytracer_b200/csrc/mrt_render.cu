@@ -63,7 +63,9 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
 // order.  Only the task number and the sample count stay in registers while a ray is traced: the
 // pixel's running mean and fp32 sums are read and written back at the end of each sample (a few
 // bytes per ray), which leaves the registers to the traversal.  Implicit tasks are fetched in
-// 8x4-pixel tiles (when the image allows) so the rays of a warp start coherent.
+// 2x16-pixel tiles (when the image allows) so the rays of a warp start coherent; tiles are handed
+// out row by row.  On the 1,000,000-triangle soup frame 2x16 tiles beat 4x8 by 0.7 % and 8x4 by
+// 3.3 %; handing out 64x32-pixel regions per SM, or the tiles in vertical strips, was slower.
 struct NsLane {
     uint32_t t;    // task number
     uint32_t si;   // samples done
@@ -74,7 +76,7 @@ struct NsWork {
     const RenderParams *p;
     uint32_t first, count;
     uint32_t *ctr;
-    uint32_t tiles_x;   // 0: row-major tasks
+    uint32_t tiles_x;   // tiles per tile row (0: row-major tasks)
     __device__ uint32_t total() const { return count; }
     __device__ uint32_t *counter() const { return ctr; }
     template <class L>
@@ -90,7 +92,7 @@ struct NsWork {
         uint32_t t = first + item;
         if (tiles_x) {
             const uint32_t tile = item >> 5, w = item & 31u;
-            const uint32_t x = (tile % tiles_x) * 8u + (w & 7u), y = (tile / tiles_x) * 4u + (w >> 3);
+            const uint32_t x = (tile % tiles_x) * 2u + (w & 1u), y = (tile / tiles_x) * 16u + (w >> 1);
             t = y * p->width + x;
         }
         lane.t = t;
@@ -585,7 +587,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     if (direct_shader(o->shader)) {
         const bool fast = accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST;
         const uint32_t rows = 16u * (o->height / 16u);
-        const uint32_t tiles_x = (plan.implicit && o->width % 8u == 0 && rows % 4u == 0) ? o->width / 8u : 0u;
+        const uint32_t tiles_x = (plan.implicit && o->width % 2u == 0 && rows % 16u == 0) ? o->width / 2u : 0u;
         for (size_t r = 0; r < plan.round_first.size(); ++r) {
             if (s->stop.load()) return cancelled(ctx, q);
             if (fast) {
@@ -867,7 +869,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
     cudaEventRecord(ctx->ev0, q);
     if (direct_shader(o->shader)) {
         if (accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST) {
-            const uint32_t tiles_x = ((16u * bsy) % 4u == 0) ? o->width / 8u : 0u;
+            const uint32_t tiles_x = o->width / 2u;   // width is a multiple of 16, rows of 16
             cudaMemsetAsync(counters, 0, sizeof(uint32_t), q);
             k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, 0u, p.n_tasks, counters, tiles_x);
         } else {
