@@ -524,6 +524,88 @@ def bench_scene(args):
     ctx.close()
 
 
+def bench_raster(args):
+    """The raster preview of the config-2 soup (1,000,000 triangles, 1920x1080): one step = one
+    mrt_raster_preview on a device bitmap; value = scene triangles / device time (Mtris/s)."""
+    import torch
+    import mobileraytracer_b200 as m
+    from mobileraytracer_b200 import scenes
+    w, h = 1920, 1080
+    sc = scenes.triangle_soup(1_000_000, 0, w, h)
+    torch.cuda.set_device(0)
+    ctx = m.Context(0)
+    scene = m.Scene(ctx, sc)
+    bitmap = torch.zeros((h, w), dtype=torch.int32, device="cuda")
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream, device="cuda")
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)   # evicts L2 before every step; not inside the timed events
+        return scene.raster_preview(sc.camera, w, h, bitmap=bitmap)[1]
+
+    clocks = ClockSampler(0).__enter__()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks.mark()
+    dev_ms, st = 0.0, None
+    for _ in range(args.steps):
+        st = step()
+        dev_ms += st.device_ms
+    torch.cuda.synchronize()
+    clocks.__exit__(None, None, None)
+    ms = dev_ms / args.steps
+    covered = int((bitmap != 0).sum().item())
+    # algorithmic bytes: 48 per triangle (A, AB, AC records), per pixel 8 (depth-key clear) + 8 (key
+    # read) + 4 (bitmap write), 8 per covered sample (the atomicMin), 4 per drawn pixel (material id)
+    algo = 48 * sc.n_triangles + 20 * w * h + 8 * st.fragments + 4 * covered
+    peak, peak_src = measured_peak()
+    achieved = algo / (ms / 1e3) / 1e9
+    host_bm = torch.zeros((h, w), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    scene.raster_preview(sc.camera, w, h, bitmap=host_bm)
+    n_e2e = max(1, min(args.e2e_steps, args.steps))
+    t1 = time.perf_counter()
+    for _ in range(n_e2e):
+        scene.raster_preview(sc.camera, w, h, bitmap=host_bm)
+    e2e_s = (time.perf_counter() - t1) / n_e2e
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import orc as O
+        try:
+            n, t = 0, 0.0
+            while t < min(args.cpu_budget, 10.0):
+                t0 = time.perf_counter()
+                O.raster_preview(sc, sc.camera, w, h)
+                t += time.perf_counter() - t0
+                n += 1
+            cpu = {"value": n * sc.n_triangles / t / 1e6, "unit": "Mtris/s", "cores": 1, "kind": "port",
+                   "sample": f"{n} whole previews by the oracle's serial restatement (the reference draws with "
+                             f"OpenGL ES, unavailable here)"}
+        except Exception as e:   # the checker library was not built
+            log(f"cpu baseline unavailable: {e}")
+    line = {
+        "metric": METRIC, "value": sc.n_triangles / (ms / 1e3) / 1e6, "unit": "Mtris/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "raster preview (MainRenderer.copyFrame) of the 1,000,000-triangle soup seed 0, "
+                               "1920x1080, the CLI camera", "triangles": sc.n_triangles, "drawn": st.drawn,
+                   "fragments": st.fragments, "covered_pixels": covered,
+                   "l2": "flushed before every step (512 MiB write outside the timed events)"},
+        "e2e": {"value": sc.n_triangles / e2e_s / 1e6, "unit": "Mtris/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": host_bm.nbytes},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": None, "algorithmic_bytes_per_launch": algo,
+                     "kernel": "k_raster_tris + k_raster_big + k_raster_resolve (+ key clear)"},
+        "clocks": clocks.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+
+
 def scene_cpu_baseline(sc, opts, rays_per_path: float, budget_s: float):
     """The reference's CPU renderer (oracle/_ref, its release optimisation level) on the host cores.
     It traces but does not count rays, so its Mrays/s is its camera paths per second times the rays
@@ -570,9 +652,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="frame", choices=["frame", "cornell", "terrain", "batched", "served"],
+    ap.add_argument("--workload", default="frame", choices=["frame", "cornell", "terrain", "batched", "served", "raster"],
                     help="frame: the 1920x1080 NoShadows frame (default); cornell / terrain: the Whitted and "
-                         "PathTracer frames; batched: the 256-job batch; served: the request stream")
+                         "PathTracer frames; batched: the 256-job batch; served: the request stream; raster: the "
+                         "raster preview of the frame's soup")
     ap.add_argument("--duration", type=float, default=120.0, help="served: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=50.0, help="served: arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: device footprint budget")
@@ -593,6 +676,9 @@ def main():
         return
     if args.workload == "served":
         bench_served(args)
+        return
+    if args.workload == "raster":
+        bench_raster(args)
         return
     if args.workload in SCENE_WORKLOADS:
         bench_scene(args)

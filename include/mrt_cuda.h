@@ -22,6 +22,11 @@
  *                         shade() (app/Components/Shaders/{NoShadows,Whitted,PathTracer}.cpp)
  *   mrt_render_stop       Renderer::stopRender()                     (app/MobileRT/Renderer.cpp:61-65)
  *   mrt_render_progress   Renderer::getSample()                      (app/MobileRT/Renderer.cpp:118-120)
+ *   mrt_raster_preview    the Android front end's raster preview: MainRenderer.copyFrame +
+ *                         copyFrameBuffer (app/src/main/java/puscas/mobilertapp/MainRenderer.java:
+ *                         111-139, 338-546) over DrawView's initVerticesArray / initColorsArray /
+ *                         initCameraArray (app/System_dependent/Android_JNI/DrawView.cpp:47-210) and
+ *                         VertexShaderRaster.glsl / FragmentShaderRaster.glsl
  * mrt_render_noalloc and the mrt_batch_* calls have no counterpart in the reference (the reference
  * renders one frame per Renderer::renderFrame call).
  */
@@ -292,6 +297,25 @@ int mrt_render_noalloc(MrtScene *scene, const MrtCamera *camera, const MrtRender
                        uint32_t stride_bytes, float *accum, MrtRenderStats *stats);
 void mrt_render_stop(MrtScene *scene);
 uint32_t mrt_render_progress(const MrtScene *scene);
+
+/* ---- raster preview ---------------------------------------------------------------------------- */
+/* The first image the Android front end shows: the scene's triangles drawn with one flat colour each
+ * (the material's max(Kd, Ks, Kt, Le) per component, or the mean of the vertex colours for a
+ * triangle without material), back faces culled, nearest surface kept (a later triangle wins a
+ * depth tie), background 0.  The camera's position, direction and up give a look-at view with z
+ * negated; Perspective cameras project with fovY = 0.918 x the vertical field of view, near 0.1,
+ * far 1e38; Orthographic ones with the film half sizes.  Pixel (x, y) of the width x height frame
+ * is written at bitmap row y from the top as R | G << 8 | B << 16 | A << 24 (the render bitmap's
+ * format).  The reference draws with OpenGL ES, which is not available to this library: parity is
+ * with the oracle's restatement of the same pipeline (no graphics driver has been run). */
+typedef struct MrtRasterStats {
+    uint64_t triangles;   /* scene triangles */
+    uint64_t drawn;       /* front-facing triangles (after near/far clipping) that reached the rasteriser */
+    uint64_t fragments;   /* pixel samples covered by them */
+    float device_ms;      /* device time of the preview */
+} MrtRasterStats;
+int mrt_raster_preview(MrtScene *scene, const MrtCamera *camera, uint32_t width, uint32_t height,
+                       uint32_t *bitmap, uint32_t stride_bytes, uint32_t mem, MrtRasterStats *stats);
 
 /* ---- batched rendering (no counterpart in the reference) ------------------------------------ */
 /* Many renders of different scenes, cameras, resolutions and spp as one stream of waves over a

@@ -206,6 +206,20 @@ class Scene:
                                            ctypes.byref(stats)), "mrt_render")
         return bitmap, accum, stats
 
+    def raster_preview(self, camera, width: int, height: int, bitmap=None, stride_bytes: int | None = None):
+        """The Android front end's raster preview of the scene's triangles (MainRenderer.copyFrame).
+        numpy buffer -> host path; CUDA tensor -> device path.  Returns (bitmap, MrtRasterStats)."""
+        if bitmap is None:
+            bitmap = np.zeros((height, width), np.uint32)
+        if stride_bytes is None:
+            stride_bytes = width * 4
+        bp, mem = _ptr(bitmap)
+        stats = capi.MrtRasterStats()
+        _after_torch(self.ctx, bitmap, None)
+        self.ctx.check(self.lib.mrt_raster_preview(self.h, ctypes.byref(camera), width, height, bp, stride_bytes, mem,
+                                                   ctypes.byref(stats)), "mrt_raster_preview")
+        return bitmap, stats
+
     def stop(self):
         self.lib.mrt_render_stop(self.h)
 

@@ -101,6 +101,11 @@ class MrtRenderStats(ctypes.Structure):
                 ("device_ms", ctypes.c_float)]
 
 
+class MrtRasterStats(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_uint64), ("drawn", ctypes.c_uint64), ("fragments", ctypes.c_uint64),
+                ("device_ms", ctypes.c_float)]
+
+
 class MrtBatchOpts(ctypes.Structure):
     _fields_ = [("wave_roots", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
                 ("blocks_per_sm", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
@@ -187,6 +192,8 @@ def load() -> ctypes.CDLL:
         "mrt_obj_free": (None, [vp]),
         "mrt_render_stop": (None, [vp]),
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
+        "mrt_raster_preview": (ctypes.c_int, [vp, P(MrtCamera), ctypes.c_uint32, ctypes.c_uint32, vp, ctypes.c_uint32,
+                                              ctypes.c_uint32, P(MrtRasterStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -203,5 +210,5 @@ EXPORTED_SYMBOLS = [
     "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress", "mrt_batch_create", "mrt_batch_destroy",
     "mrt_batch_submit", "mrt_batch_step", "mrt_batch_completed", "mrt_batch_run", "mrt_batch_stats",
     "mrt_arena_create", "mrt_arena_destroy", "mrt_arena_stats", "mrt_context_set_arena", "mrt_scene_move",
-    "mrt_obj_load", "mrt_obj_free",
+    "mrt_obj_load", "mrt_obj_free", "mrt_raster_preview",
 ]

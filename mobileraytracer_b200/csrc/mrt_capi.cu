@@ -234,6 +234,7 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto &b : ctx->scratch) dev_free(b);
     for (auto &b : ctx->wave) dev_free(b);
+    for (auto &b : ctx->raster) dev_free(b);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);

@@ -1579,3 +1579,210 @@ int orc_aabb_intersect(const float *bmin, const float *bmax, const float *o, con
     Ray r; r.origin = vld(o); r.dir = vld(d); r.depth = 1; r.exclude = MRT_HIT_NONE;
     return box_hit(&b, &r);
 }
+
+/* ================================ raster preview ==================================================
+ * The Android front end's first image (MainRenderer.copyFrame, MainRenderer.java:338-546, over
+ * DrawView.cpp:47-210 and VertexShaderRaster.glsl / FragmentShaderRaster.glsl): the scene triangles
+ * (A, A + AB, A + AC with z negated, DrawView.cpp:131-154), one colour each (DrawView.cpp:178-196),
+ * projection x view from android.opengl.Matrix (perspectiveM with fovY = 0.918 x the vertical field
+ * of view, near 0.1, far 1e38, or orthoM with the film half sizes; setLookAtM on the z-negated
+ * camera), back faces culled (CCW front), depth test LEQUAL against 1, colour cleared to 0, rows
+ * flipped on read-back (copyFrameBuffer, MainRenderer.java:111-139).  The steps OpenGL leaves to the
+ * implementation are the library's (clip near/far and a guard band of 16 w in x and y, snap to 1/256
+ * pixel, pixel centres with the top-left rule, linear window-space depth clamped to [0, 1]); this is
+ * an independent serial restatement with a literal LEQUAL depth buffer in draw order. */
+typedef struct { float m[16]; } M4;   /* column-major: (row r, column c) at m[4 c + r] */
+typedef struct { float x, y, z, w; } C4;
+
+static M4 m4_perspective(float fovy, float aspect, float zn, float zf) {
+    M4 r; memset(&r, 0, sizeof(r));
+    const float f = 1.0f / (float)tan((double)fovy * (3.14159265358979323846 / 360.0));
+    const float rr = 1.0f / (zn - zf);
+    r.m[0] = f / aspect; r.m[5] = f; r.m[10] = (zf + zn) * rr; r.m[11] = -1.0f; r.m[14] = 2.0f * zf * zn * rr;
+    return r;
+}
+static M4 m4_ortho(float l, float rt, float b, float t, float zn, float zf) {
+    M4 r; memset(&r, 0, sizeof(r));
+    const float rw = 1.0f / (rt - l), rh = 1.0f / (t - b), rd = 1.0f / (zf - zn);
+    r.m[0] = 2.0f * rw; r.m[5] = 2.0f * rh; r.m[10] = -2.0f * rd;
+    r.m[12] = -(rt + l) * rw; r.m[13] = -(t + b) * rh; r.m[14] = -(zf + zn) * rd; r.m[15] = 1.0f;
+    return r;
+}
+static float m4_len(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+static M4 m4_look_at(V3 e, V3 c, V3 u) {
+    V3 f = vsub(c, e);
+    const float rlf = 1.0f / m4_len(f.x, f.y, f.z);
+    f = v3(f.x * rlf, f.y * rlf, f.z * rlf);
+    V3 s = v3(f.y * u.z - f.z * u.y, f.z * u.x - f.x * u.z, f.x * u.y - f.y * u.x);
+    const float rls = 1.0f / m4_len(s.x, s.y, s.z);
+    s = v3(s.x * rls, s.y * rls, s.z * rls);
+    const V3 v = v3(s.y * f.z - s.z * f.y, s.z * f.x - s.x * f.z, s.x * f.y - s.y * f.x);
+    M4 r; memset(&r, 0, sizeof(r));
+    r.m[0] = s.x; r.m[1] = v.x; r.m[2] = -f.x;
+    r.m[4] = s.y; r.m[5] = v.y; r.m[6] = -f.y;
+    r.m[8] = s.z; r.m[9] = v.z; r.m[10] = -f.z;
+    r.m[15] = 1.0f;
+    for (int i = 0; i < 4; ++i) r.m[12 + i] += r.m[i] * -e.x + r.m[4 + i] * -e.y + r.m[8 + i] * -e.z;   /* translateM */
+    return r;
+}
+static M4 m4_mul(const M4 *a, const M4 *b) {
+    M4 r;
+    for (int c = 0; c < 4; ++c)
+        for (int row = 0; row < 4; ++row)
+            r.m[4 * c + row] = ((a->m[row] * b->m[4 * c] + a->m[4 + row] * b->m[4 * c + 1]) + a->m[8 + row] * b->m[4 * c + 2]) +
+                               a->m[12 + row] * b->m[4 * c + 3];
+    return r;
+}
+static C4 ras_clip(const M4 *m, V3 p) {
+    C4 c;
+    c.x = ((m->m[0] * p.x + m->m[4] * p.y) + m->m[8] * p.z) + m->m[12];
+    c.y = ((m->m[1] * p.x + m->m[5] * p.y) + m->m[9] * p.z) + m->m[13];
+    c.z = ((m->m[2] * p.x + m->m[6] * p.y) + m->m[10] * p.z) + m->m[14];
+    c.w = ((m->m[3] * p.x + m->m[7] * p.y) + m->m[11] * p.z) + m->m[15];
+    return c;
+}
+static float ras_plane(C4 v, int p) {
+    switch (p) {
+        case 0: return v.z + v.w;
+        case 1: return v.w - v.z;
+        case 2: return 16.0f * v.w - v.x;
+        case 3: return 16.0f * v.w + v.x;
+        case 4: return 16.0f * v.w - v.y;
+        default: return 16.0f * v.w + v.y;
+    }
+}
+static int64_t ras_edge(int64_t xa, int64_t ya, int64_t xb, int64_t yb, int64_t px, int64_t py) {
+    return (xb - xa) * (py - ya) - (yb - ya) * (px - xa);
+}
+static int ras_owns(int64_t xa, int64_t ya, int64_t xb, int64_t yb) { return yb < ya || (yb == ya && xb < xa); }
+static int64_t ras_floor256(int64_t a) { return a >= 0 ? a / 256 : -((-a + 255) / 256); }
+static uint32_t ras_unorm8(float c) {
+    const float k = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+    return (uint32_t)(k * 255.0f + 0.5f);
+}
+
+int orc_raster_preview(const MrtSceneDesc *d, const MrtCamera *cam, uint32_t width, uint32_t height, uint32_t *bitmap,
+                       uint32_t stride_bytes, uint64_t *counts) {
+    if (!d || !cam || !bitmap || width == 0 || height == 0 || stride_bytes < 4u * width) return 1;
+    const Cam k = cam_make(cam);
+    const V3 eye = v3(k.position.x, k.position.y, -k.position.z);
+    const V3 dir = v3(k.direction.x, k.direction.y, -k.direction.z);
+    const V3 up = v3(k.up.x, k.up.y, -k.up.z);
+    M4 proj;
+    if (cam->kind == MRT_CAMERA_ORTHOGRAPHIC) {
+        proj = m4_ortho(-k.hfov / 2, k.hfov / 2, -k.vfov / 2, k.vfov / 2, 0.1f, 1.0e38f);
+    } else {
+        const float pi = 3.14159265358979323846f;
+        const float w = (float)width, h = (float)height;
+        const float ratio = (w / h) < (h / w) ? (h / w) : (w / h);
+        const float hf = width > height ? ratio : 1.0f, vf = width < height ? ratio : 1.0f;
+        float fovy = (k.vfov / pi) * 180.0f;
+        fovy *= 0.918f;
+        proj = m4_perspective(fovy, hf > vf ? hf : 1.0f / vf, 0.1f, 1.0e38f);
+    }
+    const M4 view = m4_look_at(eye, vadd(eye, dir), up);
+    const M4 m = m4_mul(&proj, &view);
+    const size_t npx = (size_t)width * height;
+    float *depth = (float *)malloc(sizeof(float) * npx);
+    int64_t *win = (int64_t *)malloc(sizeof(int64_t) * npx);
+    if (!depth || !win) { free(depth); free(win); return 2; }
+    for (size_t i = 0; i < npx; ++i) { depth[i] = 1.0f; win[i] = -1; }
+    const float hw = 0.5f * (float)width, hh = 0.5f * (float)height;
+    uint64_t drawn = 0, frags = 0;
+    for (uint32_t i = 0; i < d->n_triangles; ++i) {
+        const float *t = d->tri_abc + 9 * (size_t)i;
+        const V3 A = vld(t), AB = vsub(vld(t + 3), A), AC = vsub(vld(t + 6), A);   /* Triangle.cpp: AB, AC */
+        C4 poly[9], tmp[9];
+        poly[0] = ras_clip(&m, v3(A.x, A.y, -A.z));
+        poly[1] = ras_clip(&m, v3(A.x + AB.x, A.y + AB.y, -(A.z + AB.z)));
+        poly[2] = ras_clip(&m, v3(A.x + AC.x, A.y + AC.y, -(A.z + AC.z)));
+        int n = 3;
+        for (int p = 0; p < 6 && n >= 3; ++p) {
+            int out = 0;
+            for (int q = 0; q < n; ++q) {
+                const C4 S = poly[q], E = poly[(q + 1) % n];
+                const float ds = ras_plane(S, p), de = ras_plane(E, p);
+                if (ds >= 0.0f) tmp[out++] = S;
+                if ((ds >= 0.0f) != (de >= 0.0f)) {
+                    const float u = ds / (ds - de);
+                    C4 c; c.x = S.x + u * (E.x - S.x); c.y = S.y + u * (E.y - S.y); c.z = S.z + u * (E.z - S.z);
+                    c.w = S.w + u * (E.w - S.w);
+                    tmp[out++] = c;
+                }
+            }
+            n = out;
+            memcpy(poly, tmp, sizeof(C4) * (size_t)n);
+        }
+        if (n < 3) continue;
+        int64_t X[9], Y[9];
+        float Z[9];
+        for (int q = 0; q < n; ++q) {
+            const float xn = poly[q].x / poly[q].w, yn = poly[q].y / poly[q].w, zn = poly[q].z / poly[q].w;
+            X[q] = (int64_t)lrintf((hw * xn + hw) * 256.0f);
+            Y[q] = (int64_t)lrintf((hh * yn + hh) * 256.0f);
+            Z[q] = 0.5f * zn + 0.5f;
+        }
+        for (int f = 1; f + 1 < n; ++f) {
+            const int v[3] = {0, f, f + 1};
+            const int64_t x0 = X[v[0]], y0 = Y[v[0]], x1 = X[v[1]], y1 = Y[v[1]], x2 = X[v[2]], y2 = Y[v[2]];
+            const float z0 = Z[v[0]], z1 = Z[v[1]], z2 = Z[v[2]];
+            const int64_t area2 = ras_edge(x0, y0, x1, y1, x2, y2);
+            if (area2 <= 0) continue;
+            ++drawn;
+            const int o12 = ras_owns(x1, y1, x2, y2), o20 = ras_owns(x2, y2, x0, y0), o01 = ras_owns(x0, y0, x1, y1);
+            const float inv = 1.0f / (float)area2;
+            const int64_t xmin = x0 < x1 ? (x0 < x2 ? x0 : x2) : (x1 < x2 ? x1 : x2);
+            const int64_t xmax = x0 > x1 ? (x0 > x2 ? x0 : x2) : (x1 > x2 ? x1 : x2);
+            const int64_t ymin = y0 < y1 ? (y0 < y2 ? y0 : y2) : (y1 < y2 ? y1 : y2);
+            const int64_t ymax = y0 > y1 ? (y0 > y2 ? y0 : y2) : (y1 > y2 ? y1 : y2);
+            int64_t px0 = -ras_floor256(-(xmin - 128)), px1 = ras_floor256(xmax - 128);
+            int64_t py0 = -ras_floor256(-(ymin - 128)), py1 = ras_floor256(ymax - 128);
+            px0 = px0 < 0 ? 0 : px0;
+            py0 = py0 < 0 ? 0 : py0;
+            px1 = px1 > (int64_t)width - 1 ? (int64_t)width - 1 : px1;
+            py1 = py1 > (int64_t)height - 1 ? (int64_t)height - 1 : py1;
+            for (int64_t py = py0; py <= py1; ++py)
+                for (int64_t px = px0; px <= px1; ++px) {
+                    const int64_t cx = px * 256 + 128, cy = py * 256 + 128;
+                    const int64_t w0 = ras_edge(x1, y1, x2, y2, cx, cy), w1 = ras_edge(x2, y2, x0, y0, cx, cy),
+                                  w2 = ras_edge(x0, y0, x1, y1, cx, cy);
+                    if (!((w0 > 0 || (w0 == 0 && o12)) && (w1 > 0 || (w1 == 0 && o20)) && (w2 > 0 || (w2 == 0 && o01))))
+                        continue;
+                    float z = z0 + ((float)w1 * (z1 - z0) + (float)w2 * (z2 - z0)) * inv;
+                    if (!(z > 0.0f)) z = 0.0f;
+                    if (z > 1.0f) z = 1.0f;
+                    ++frags;
+                    const size_t at = (size_t)py * width + (size_t)px;
+                    if (z <= depth[at]) { depth[at] = z; win[at] = i; }   /* GL_LEQUAL in draw order */
+                }
+        }
+    }
+    const uint32_t stride = stride_bytes / 4u;
+    for (uint32_t y = 0; y < height; ++y)
+        for (uint32_t x = 0; x < width; ++x) {
+            const int64_t tri = win[(size_t)y * width + x];
+            uint32_t out = 0u;
+            if (tri >= 0) {
+                const int32_t mi = d->tri_material ? d->tri_material[tri] : -1;
+                V3 c;
+                if (mi >= 0 && (uint32_t)mi < d->n_materials) {   /* glm::max(x, y) = x < y ? y : x */
+                    const MrtMaterial *mt = &d->materials[mi];
+                    c = vld(mt->kd);
+                    c = v3(mt->ks[0] < c.x ? c.x : mt->ks[0], mt->ks[1] < c.y ? c.y : mt->ks[1], mt->ks[2] < c.z ? c.z : mt->ks[2]);
+                    c = v3(mt->kt[0] < c.x ? c.x : mt->kt[0], mt->kt[1] < c.y ? c.y : mt->kt[1], mt->kt[2] < c.z ? c.z : mt->kt[2]);
+                    c = v3(mt->le[0] < c.x ? c.x : mt->le[0], mt->le[1] < c.y ? c.y : mt->le[1], mt->le[2] < c.z ? c.z : mt->le[2]);
+                } else if (d->tri_colors) {
+                    const float *k3 = d->tri_colors + 9 * (size_t)tri;
+                    c = v3(((k3[0] + k3[3]) + k3[6]) / 3.0f, ((k3[1] + k3[4]) + k3[7]) / 3.0f, ((k3[2] + k3[5]) + k3[8]) / 3.0f);
+                } else {
+                    c = v3(0.0f, 0.0f, 0.0f);
+                }
+                out = ras_unorm8(c.x) | (ras_unorm8(c.y) << 8) | (ras_unorm8(c.z) << 16) | (255u << 24);
+            }
+            bitmap[(size_t)(height - 1 - y) * stride + x] = out;
+        }
+    free(depth);
+    free(win);
+    if (counts) { counts[0] = drawn; counts[1] = frags; }
+    return 0;
+}

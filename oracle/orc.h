@@ -66,6 +66,10 @@ int orc_plane_intersect(const float *pn, const float *o, const float *d, float l
 int orc_sphere_intersect(const float *cr, const float *o, const float *d, float length, float *out_t, float *out_n);
 int orc_sphere_intersect_box(const float *cr, const float *bmin, const float *bmax);
 int orc_aabb_intersect(const float *bmin, const float *bmax, const float *o, const float *d);
+/* raster preview of the scene triangles (MainRenderer.copyFrame); counts[0] = triangles drawn after
+ * clipping, counts[1] = covered pixel samples; 0 on success */
+int orc_raster_preview(const MrtSceneDesc *d, const MrtCamera *cam, uint32_t width, uint32_t height, uint32_t *bitmap,
+                       uint32_t stride_bytes, uint64_t *counts);
 float orc_aabb_area(const float *bmin, const float *bmax);
 float orc_halton(uint32_t index, uint32_t base);
 uint32_t orc_incremental_avg(const float *rgb, uint32_t avg, uint32_t n);

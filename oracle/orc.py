@@ -61,6 +61,7 @@ def orc() -> ctypes.CDLL:
             "orc_camera_ray": (None, [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, fp]),
             "orc_sample": (ctypes.c_float, [vp, ip, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
             "orc_sincos": (None, [ctypes.c_float, fp, fp]),
+            "orc_raster_preview": (ip, [vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp, ctypes.c_uint32, vp]),
         })
         _orc = lib
     return _orc
@@ -122,6 +123,17 @@ def make_rays(origins: np.ndarray, dirs: np.ndarray, depth: int = 1, exclude=Non
     r["depth"] = depth
     r["exclude"] = 0xFFFFFFFF if exclude is None else exclude
     return r
+
+
+def raster_preview(scene, camera, width: int, height: int):
+    """The restatement of the raster preview: (bitmap uint32 [height, width], drawn, fragments)."""
+    desc = scene.desc()
+    bm = np.zeros((height, width), np.uint32)
+    counts = np.zeros(2, np.uint64)
+    st = orc().orc_raster_preview(ctypes.byref(desc), ctypes.byref(camera), width, height, bm.ctypes.data, width * 4,
+                                  counts.ctypes.data)
+    assert st == 0, st
+    return bm, int(counts[0]), int(counts[1])
 
 
 class OrcScene:
