@@ -515,7 +515,7 @@ def bench_scene(args):
                    "samples_per_s": paths / (dev_ms / 1e3), "bvh_build_seconds": build_s,
                    "l2": "flushed before every step (512 MiB write outside the timed events)"},
         "e2e": {"value": rays / args.steps / e2e_s / 1e6, "unit": "Mrays/s",
-                "h2d_bytes_per_step": host_bm.nbytes + host_acc.nbytes,
+                "h2d_bytes_per_step": host_bm.nbytes - 4 * w * 16 * (h // 16) + host_acc.nbytes,
                 "d2h_bytes_per_step": host_bm.nbytes + host_acc.nbytes},
         "gpu_launches": None, "roofline": None, "clocks": clocks.summary(), "cpu_baseline": cpu,
     }
@@ -774,7 +774,10 @@ def main():
         "config": {"workload": WORKLOAD, "rays_per_step": rays_per_step, "rows_rendered": 16 * (HEIGHT // 16),
                    "l2": "flushed before every step (512 MiB write outside the timed events)",
                    "bvh_build_seconds": build_s, "wall_seconds_timed_loop": wall, "parallelism": f"replicas x{ws}"},
-        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": bm_bytes + 64 + 100,
+        # in: the bitmap rows the block schedule leaves alone (a first pass overwrites the rest without
+        # reading it), camera and options; out: the whole bitmap
+        "e2e": {"value": e2e_value, "unit": "Mrays/s",
+                "h2d_bytes_per_step": bm_bytes - 4 * WIDTH * 16 * (HEIGHT // 16) + 64 + 100,
                 "d2h_bytes_per_step": bm_bytes},
         "gpu_launches": args.steps,
         "roofline": roof,

@@ -731,7 +731,19 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
         if (st != MRT_OK) return st;
         d_bitmap = (uint32_t *)ctx->wave[7].ptr;
         d_accum = accum ? (float *)((char *)ctx->wave[7].ptr + acc_offset) : nullptr;
-        st = cuda_status(ctx, cudaMemcpyAsync(d_bitmap, bitmap, bm_bytes, cudaMemcpyHostToDevice, ctx->stream), "bitmap in");
+        // The first samples of a frame (spp_offset 0) on the plain rectangle (row pitch = 4 * width)
+        // replace every pixel they render without reading it: incrementalAvg with n = 1
+        // (Utils.cpp:48-70) keeps nothing of the old value.  Only the rows below the block schedule
+        // (height mod 16 of them, Renderer.cpp:20-21) then need the caller's bytes.
+        size_t in_from = 0;
+        if (o->spp_offset == 0 && stride_bytes == 4u * o->width) {
+            const TaskPlan &plan = *cached_plan(s, o->width, o->height, o->width);
+            if (plan.n_tasks > 0 && plan.implicit) in_from = 4ull * plan.n_tasks;
+        }
+        if (in_from < bm_bytes)
+            st = cuda_status(ctx, cudaMemcpyAsync((char *)d_bitmap + in_from, (const char *)bitmap + in_from,
+                                                  bm_bytes - in_from, cudaMemcpyHostToDevice, ctx->stream),
+                             "bitmap in");
         if (st == MRT_OK && accum)
             st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");
         if (st != MRT_OK) return st;

@@ -127,6 +127,31 @@ def test_odd_sizes_and_stride(ctx):
     assert (padded[:, :64] == plain).all() and (padded[:, 64:] == 0xDEADBEEF).all()
 
 
+def test_host_path_keeps_unrendered_rows(ctx):
+    """Host buffers: a first pass (spp_offset 0) copies in only the rows below the block schedule,
+    since it overwrites the rest without reading it; a continuation (spp_offset > 0) reads them all.
+    Either way the host result equals the device path started from the same bitmap."""
+    torch = pytest.importorskip("torch")
+    sc = scenes.glass_room()
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH)
+    # 152 = 16 * 9 + 8 with 152 / 9 = 16 blocks down: the plain rectangle of rows 0..143; rows
+    # 144..151 are not rendered (as rows 1072..1079 of a 1080-row frame)
+    w, h = 96, 152
+    rng = np.random.default_rng(3)
+    start = rng.integers(0, 2**32, size=(h, w), dtype=np.uint32)
+    for shader, spp_offset in ((NS, 0), (PT, 0), (NS, 1), (PT, 2)):
+        opts = capi.render_opts(shader=shader, width=w, height=h, spp=2, spl=1, seed=7, spp_offset=spp_offset)
+        host = start.copy()
+        g.render(sc.camera, opts, bitmap=host)
+        dev = torch.from_numpy(start.view(np.int32).copy()).cuda()
+        g.render(sc.camera, opts, bitmap=dev)
+        torch.cuda.synchronize()
+        assert (host == dev.cpu().numpy().view(np.uint32)).all(), (shader, spp_offset)
+        assert (host[144:] == start[144:]).all()
+        assert (host[:144] != start[:144]).any()
+    g.close()
+
+
 def test_errors_are_reported(ctx):
     import mobileraytracer_b200 as m
     sc = scenes.glass_room()
