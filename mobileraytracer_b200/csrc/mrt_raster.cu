@@ -427,7 +427,9 @@ extern "C" int mrt_raster_preview(MrtScene *s, const MrtCamera *cam, uint32_t wi
     cudaSetDevice(ctx->device);
     cudaStream_t q = ctx->stream;
     const size_t pixels = (size_t)width * height;
-    const uint32_t big_cap = s->n_tri + 1024u;
+    // queue room for every triangle of scenes up to 2^20 triangles (58 MB); beyond that, large
+    // triangles that find the queue full are covered by their own thread (same result, slower)
+    const uint32_t big_cap = std::min<uint32_t>(s->n_tri, 1u << 20) + 1024u;
     int st = ensure(ctx, ctx->raster[0], 8 * pixels);
     if (st == MRT_OK) st = ensure(ctx, ctx->raster[1], sizeof(RasterTri) * (size_t)big_cap);
     if (st == MRT_OK) st = ensure(ctx, ctx->raster[2], 4 * sizeof(unsigned long long));
