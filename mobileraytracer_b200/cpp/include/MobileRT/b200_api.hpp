@@ -228,6 +228,10 @@ public:
     void renderFrame(std::uint32_t *bitmap, std::int32_t numThreads, std::uint32_t stride) noexcept;
     void stopRender() noexcept;             // Renderer.cpp:61-65, callable from another thread
     std::uint32_t getSample() const noexcept;   // Renderer.cpp:118-120
+    // the Android front end's first image of this renderer's scene and camera (DrawView.cpp:47-210
+    // arrays drawn by MainRenderer.copyFrame, MainRenderer.java:338-546): flat-coloured triangles,
+    // back faces culled, nearest surface kept, background 0, same bitmap format as renderFrame
+    void rasterPreview(std::uint32_t *bitmap, std::uint32_t stride) noexcept;
 
     // extensions: stream key, Russian-roulette depths, last failure
     void setSeed(std::uint64_t seed) noexcept { seed_ = seed; }

@@ -204,6 +204,20 @@ void Renderer::stopRender() noexcept {
     if (shader_ && shader_->device_) mrt_render_stop(shader_->device_->scene);
 }
 
+void Renderer::rasterPreview(std::uint32_t *bitmap, std::uint32_t stride) noexcept {
+    if (!shader_ || !shader_->device_) {
+        error_ = shader_ ? shader_->error_ : "no shader";
+        std::fprintf(stderr, "MobileRT: rasterPreview without an uploaded scene: %s\n", error_.c_str());
+        return;
+    }
+    const MrtCamera c = to_mrt(*camera_);
+    const int st = mrt_raster_preview(shader_->device_->scene, &c, width_, height_, bitmap, stride, MRT_MEM_HOST, nullptr);
+    if (st != MRT_OK) {
+        error_ = context_error(context(), st, "mrt_raster_preview");
+        std::fprintf(stderr, "MobileRT: %s\n", error_.c_str());
+    }
+}
+
 std::uint32_t Renderer::getSample() const noexcept {
     return (shader_ && shader_->device_) ? mrt_render_progress(shader_->device_->scene) : 0u;
 }

@@ -50,7 +50,7 @@ MobileRT::Material material() {
 }  // namespace
 
 int main(int argc, char **argv) {
-    if (argc != 3) { std::fprintf(stderr, "usage: %s scene.bin out.bin\n", argv[0]); return 1; }
+    if (argc != 3 && argc != 4) { std::fprintf(stderr, "usage: %s scene.bin out.bin [preview.bin]\n", argv[0]); return 1; }
     in = std::fopen(argv[1], "rb");
     if (!in) return 1;
     MobileRT::Scene scene{};
@@ -113,6 +113,14 @@ int main(int argc, char **argv) {
     FILE *out = std::fopen(argv[2], "wb");
     std::fwrite(bitmap.data(), sizeof(uint32_t), bitmap.size(), out);
     std::fclose(out);
+    if (argc == 4) {   // the front end's raster preview of the same renderer
+        std::vector<uint32_t> preview(static_cast<size_t>(w) * h, 0u);
+        renderer.rasterPreview(preview.data(), w * sizeof(uint32_t));
+        if (!renderer.lastError().empty()) { std::fprintf(stderr, "%s\n", renderer.lastError().c_str()); return 4; }
+        FILE *pv = std::fopen(argv[3], "wb");
+        std::fwrite(preview.data(), sizeof(uint32_t), preview.size(), pv);
+        std::fclose(pv);
+    }
     std::printf("rendered %ux%u, samples %u\n", w, h, renderer.getSample());
     return 0;
 }

@@ -76,13 +76,17 @@ def client(tmp_path_factory):
 def test_renderframe_through_the_dropin(ctx, client, tmp_path, shader, accel, mode):
     for sc in (scenes.glass_room(), scenes.cornell_box()):
         opts = capi.render_opts(shader=shader, width=80, height=48, spp=2, spl=1)
-        path, out = str(tmp_path / "scene.bin"), str(tmp_path / "out.bin")
+        path, out, pv = str(tmp_path / "scene.bin"), str(tmp_path / "out.bin"), str(tmp_path / "preview.bin")
         _write_scene(path, sc, opts, accel, mode)
-        r = subprocess.run([client, path, out], capture_output=True, text=True)
+        r = subprocess.run([client, path, out, pv], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
         got = np.fromfile(out, np.uint32).reshape(48, 80)
-        want, _, _ = Scene(ctx, sc).build(accel, mode).render(sc.camera, opts)
+        g = Scene(ctx, sc).build(accel, mode)
+        want, _, _ = g.render(sc.camera, opts)
         assert (got == want).all()
+        # Renderer::rasterPreview (the front end's first image) equals the C ABI's preview
+        want_pv, _ = g.raster_preview(sc.camera, 80, 48)
+        assert (np.fromfile(pv, np.uint32).reshape(48, 80) == want_pv).all()
 
 
 @pytest.fixture(scope="module")
