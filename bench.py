@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 
 WIDTH, HEIGHT, N_TRI, SEED = 1920, 1080, 1_000_000, 0
 METRIC = "Mrays/s @1 B200, batched+served vs plain GPU vs host CPU; p50/p99 job latency"
-WORKLOAD = ("config 2: NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point light, "
+WORKLOAD = ("NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point light, "
             "BVH built on the device")
 
 
@@ -128,7 +128,7 @@ def measured_peak():
 
 def profiled_traffic_per_ray():
     """DRAM bytes per ray of the render kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "render_noshadows_config2.md")
+    p = os.path.join(ROOT, "profiles", "render_noshadows_soup_1080p.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -215,7 +215,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-BATCH_WORKLOAD = ("config 4: 256 PathTracer jobs (depth 6, Russian roulette beyond depth 3, 1 light sample), "
+BATCH_WORKLOAD = ("256 PathTracer jobs (depth 6, Russian roulette beyond depth 3, 1 light sample), "
                   "job i = triangle soup of seed i with N log-uniform over [1e3, 2e6], 4 area-light quads of "
                   "emission 10, square image of side log-uniform over [128, 1024] (multiple of 16), spp uniform "
                   "over {1, 4, 16, 64}")
@@ -254,7 +254,7 @@ def job_opts(job, capi, spp_offset: int = 0, spp: int | None = None):
 
 
 def bench_batched(args):
-    """Config 4: the batched renderer against the plain one-job-per-launch renderer on the same job
+    """The 256-job batch: the batched renderer against the plain one-job-per-launch renderer on the same job
     list.  One step = every job rendered once; value = rays traced / wall time of the step."""
     from mobileraytracer_b200 import scenes
     jobs = scenes.batched_jobs(args.jobs)
@@ -349,14 +349,14 @@ def bench_batched(args):
     ctx.close()
 
 
-SERVE_WORKLOAD = ("config 5: Poisson stream of render requests, each drawn as a batched-workload job (PathTracer "
+SERVE_WORKLOAD = ("Poisson stream of render requests, each drawn as a batched-workload job (PathTracer "
                   "depth 6, soup geometry from the 256-job pool, side log-uniform over [128, 1024], spp uniform "
                   "over {1, 4, 16, 64}); 20% re-render one of the last 64 new scenes with +16 spp progressive "
                   "accumulation; admission by device footprint")
 
 
 def bench_served(args):
-    """Config 5: the same request stream served by the batched renderer (continuous batching) and by
+    """The request stream: the same requests served by the batched renderer (continuous batching) and by
     one mrt_render call per request; throughput, p50/p99 latency, offered vs achieved load."""
     from mobileraytracer_b200 import scenes
     from mobileraytracer_b200 import serve
@@ -433,9 +433,9 @@ def bench_served(args):
 
 
 SCENE_WORKLOADS = {
-    "cornell": ("config 1: Whitted 256x256, 1 spp (Constant 0.5 camera sampler), procedural Cornell box "
+    "cornell": ("Whitted 256x256, 1 spp (Constant 0.5 camera sampler), procedural Cornell box "
                 "(10 wall + 24 box triangles, mirror sphere, 2 area-light triangles of emission 15), BVH"),
-    "terrain": ("config 3: PathTracer 1024x1024, 64 spp HaltonSeq (camera, light and roulette), depth 6 with "
+    "terrain": ("PathTracer 1024x1024, 64 spp HaltonSeq (camera, light and roulette), depth 6 with "
                 "Russian roulette beyond depth 3, 512x512 fBm heightfield (524,288 triangles), 4 area-light quads "
                 "of emission 10, fp32 sums"),
 }
@@ -525,7 +525,7 @@ def bench_scene(args):
 
 
 def bench_raster(args):
-    """The raster preview of the config-2 soup (1,000,000 triangles, 1920x1080): one step = one
+    """The raster preview of the 1920x1080 frame's soup (1,000,000 triangles, 1920x1080): one step = one
     mrt_raster_preview on a device bitmap; value = scene triangles / device time (Mtris/s)."""
     import torch
     import mobileraytracer_b200 as m

@@ -196,7 +196,7 @@ def _box(lo, hi):
 
 
 def cornell_box() -> Scene:
-    """Config 1: unit Cornell box centred at the origin, open towards the camera (-z)."""
+    """Unit Cornell box centred at the origin, open towards the camera (-z)."""
     white, red, green = 0, 1, 2
     mats = [
         _material(kd=(0.73, 0.73, 0.73)),
@@ -257,7 +257,7 @@ def _soup_geometry(n: int, seed: int) -> np.ndarray:
 
 
 def triangle_soup(n: int = 1_000_000, seed: int = 0, width: int = 1920, height: int = 1080) -> Scene:
-    """Config 2: triangle soup with one white diffuse material and one point light."""
+    """Triangle soup with one white diffuse material and one point light."""
     s = Scene()
     s.tri_abc = _soup_geometry(n, seed)
     s.tri_material = np.zeros(n, np.int32)
@@ -288,7 +288,7 @@ def _value_noise(x: np.ndarray, z: np.ndarray, seed: int, octave: int) -> np.nda
 
 def heightfield(cells: int = 512, seed: int = 1, octaves: int = 6, gain: float = 0.5, lacunarity: float = 2.0,
                 amplitude: float = 0.35, width: int = 1024, height: int = 1024) -> Scene:
-    """Config 3: fBm value-noise terrain over [-1,1]^2 (2*cells^2 triangles), grey albedo per
+    """fBm value-noise terrain over [-1,1]^2 (2*cells^2 triangles), grey albedo per
     triangle ~ U[0.2, 0.8] carried in the triangle colours (material -1, NoShadows.cpp:35-36
     kD = primitive colour), 4 area-light quads (8 AreaLight triangles) of emission 10."""
     g = np.linspace(-1.0, 1.0, cells + 1)
@@ -350,7 +350,7 @@ class Job:
 
 def batched_jobs(count: int = 256, n_min: float = 1e3, n_max: float = 2e6, side_min: int = 128,
                  side_max: int = 1024, spps=(1, 4, 16, 64)) -> list[Job]:
-    """Config 4 job list: job i uses seed i; N ~ log-uniform[n_min, n_max]; image side
+    """Batched job list: job i uses seed i; N ~ log-uniform[n_min, n_max]; image side
     ~ log-uniform[side_min, side_max] rounded down to a multiple of 16 (the reference's block
     schedule covers exactly such images, Renderer.cpp:20-21); spp uniform over `spps`."""
     jobs = []

@@ -60,8 +60,8 @@ def test_glass_room_all_shaders(ctx, shader, accel, mode, oacc):
     assert stats.rays_closest == counts[0] and stats.rays_shadow == counts[1]
 
 
-def test_config1_cornell_whitted(ctx):
-    """Config 1: Whitted, 256x256, 1 spp, Constant(0.5) camera sampler, BVH."""
+def test_cornell_whitted_256(ctx):
+    """Cornell box, Whitted, 256x256, 1 spp, Constant(0.5) camera sampler, BVH."""
     sc = scenes.cornell_box()
     opts = capi.render_opts(shader=WH, width=256, height=256, spp=1, spl=1, seed=1)
     for accel, mode, oacc in ((capi.MRT_ACCEL_BVH, capi.MRT_BVH_REFERENCE, 2), (capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST, 3)):
@@ -72,7 +72,7 @@ def test_config1_cornell_whitted(ctx):
 
 @pytest.mark.parametrize("sampler", [capi.MRT_SAMPLER_STRATIFIED, capi.MRT_SAMPLER_HALTON, capi.MRT_SAMPLER_RANDOM])
 def test_pathtracer_samplers_rr(ctx, sampler):
-    """PathTracer with Russian roulette beyond depth 3, max depth 6 (config 3's setting) and every
+    """PathTracer with Russian roulette beyond depth 3, max depth 6 (the terrain frame's setting) and every
     sampler kind on the camera jitter, the light positions and the roulette."""
     sc = scenes.cornell_box()
     opts = capi.render_opts(shader=PT, width=64, height=64, spp=8, spl=1, pixel_sampler=sampler,
@@ -82,8 +82,8 @@ def test_pathtracer_samplers_rr(ctx, sampler):
     assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3)
 
 
-def test_config3_heightfield_crop(ctx):
-    """Config 3 scene (524,288-triangle fBm terrain, 4 area quads) at 64x64, 4 spp HaltonSeq,
+def test_terrain_pathtracer_crop(ctx):
+    """The terrain scene (524,288-triangle fBm terrain, 4 area quads) at 64x64, 4 spp HaltonSeq,
     depth 6, RR after 3: per-pixel radiance within 1e-3 of the oracle (asserted: exact)."""
     sc = scenes.heightfield(512, 1, width=64, height=64)
     opts = capi.render_opts(shader=PT, width=64, height=64, spp=4, spl=1, pixel_sampler=capi.MRT_SAMPLER_HALTON,

@@ -112,7 +112,7 @@ def test_host_and_device_buffers_agree(ctx):
 
 
 @pytest.mark.slow
-def test_config2_soup_camera_rays(ctx):
+def test_soup_1080p_camera_rays(ctx):
     """1,000,000-triangle soup (seed 0), 1920x1080 camera rays (every 97th pixel): FAST BVH hit ids
     equal the exact closest hit; grid at G = 128 (the reference's rule) and at G = 100 (cbrt(N),
     with the reference's shift indexing) equal the restated grid bit for bit."""
