@@ -87,3 +87,22 @@ def test_invalid_arguments(ctx):
     with pytest.raises(MrtError):
         g.raster_preview(sc.camera, 9000, 64)
     g.close()
+
+
+def test_pixel_centre_edges_and_guard_band(ctx):
+    # shared edges exactly through pixel centres (the top-left rule decides) and a triangle reaching
+    # far beyond the guard band: the device equals the restatement bit for bit
+    cam = scenes.orthographic((0.0, 0.0, -3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 16.0, 16.0)
+    ring = [(-3.875, -3.875), (3.875, -3.875), (3.875, 3.875), (-3.875, 3.875)]
+    sc = scenes.Scene()
+    sc.tri_abc = np.asarray([[0.125, 0.125, 0.0, *ring[k], 0.0, *ring[(k + 1) % 4], 0.0] for k in range(4)], np.float32)
+    sc.tri_material = np.full(4, -1, np.int32)
+    sc.tri_colors = np.asarray([[1, 0, 0] * 3, [0, 1, 0] * 3, [1, 0, 0] * 3, [0, 1, 0] * 3], np.float32)
+    bm, st = _check(ctx, sc, cam, 32, 32)
+    assert st.fragments == 31 * 31
+    big = scenes.Scene()
+    big.tri_abc = np.asarray([[-500, -500, 0, 500, -500, 0, 0, 500, 0]], np.float32)
+    big.tri_material = np.full(1, -1, np.int32)
+    big.tri_colors = np.asarray([[1, 0, 0] * 3], np.float32)
+    bm, st = _check(ctx, big, scenes.camera((0.0, 0.0, -3.0), (0.0, 0.0, 0.0)), 40, 30)
+    assert st.fragments == 40 * 30

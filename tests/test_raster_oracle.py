@@ -101,3 +101,32 @@ def test_orthographic_and_empty_scene():
     assert drawn == 1 and 31 <= len(cols) <= 33
     bm, drawn, frags = preview(scene(np.zeros((0, 9), np.float32)), 16, 16)
     assert drawn == 0 and frags == 0 and not bm.any()
+
+
+def test_guard_band_and_degenerate_triangles():
+    # a triangle reaching far outside the view in x and y (clipped by the guard band) still covers
+    # every pixel of the frame it spans; a zero-area triangle draws nothing
+    big = [-500, -500, 0, 500, -500, 0, 0, 500, 0]
+    bm, drawn, frags = preview(scene(big, RED), 40, 30)
+    assert drawn >= 1 and frags == 40 * 30 and (bm == PX_RED).all()
+    flat = [-1, 0, 0, 1, 0, 0, 0.5, 0, 0]
+    bm, drawn, frags = preview(scene(flat, RED))
+    assert drawn == 0 and frags == 0 and not bm.any()
+
+
+def test_edges_through_pixel_centres_are_owned_once():
+    # an orthographic view whose pixel centres sit on the lines x = k / 4 (k odd) with the film
+    # matched to the frame: a fan of triangles whose shared edges pass exactly through pixel centres
+    cam = scenes.orthographic((0.0, 0.0, -3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 16.0, 16.0)
+    # view spans [-4, 4] over 32 pixels: centres at -4 + (i + 0.5) / 4
+    c = (0.125, 0.125, 0.0)
+    ring = [(-3.875, -3.875), (3.875, -3.875), (3.875, 3.875), (-3.875, 3.875)]
+    tris = []
+    for k in range(4):
+        a, b = ring[k], ring[(k + 1) % 4]
+        tris.append([c[0], c[1], 0.0, a[0], a[1], 0.0, b[0], b[1], 0.0])
+    cols = [RED, GREEN, RED, GREEN]
+    bm, drawn, frags = preview(scene(tris, cols), 32, 32, cam)
+    assert drawn == 4
+    assert frags == int((bm != 0).sum())   # every covered centre belongs to exactly one triangle
+    assert frags == 31 * 31                # the square's centres, edges included once
