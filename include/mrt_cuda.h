@@ -272,7 +272,9 @@ int mrt_trace_closest(MrtScene *scene, const MrtRay *rays, uint32_t n, MrtHit *h
 /* occluded[i] = 1 if any plane/sphere/triangle blocks rays[i] within (Epsilon, dist[i]) */
 int mrt_trace_any(MrtScene *scene, const MrtRay *rays, const float *dist, uint32_t n,
                   uint8_t *occluded, uint32_t mem);
-/* Counting replay of mrt_trace_closest: per-ray node records and triangle records fetched. */
+/* Counting replay of mrt_trace_closest: per ray, on the FAST BVH the 32-byte child records and the
+ * 48-byte triangle records fetched; on the regular grid the cells visited (node_fetch) and the
+ * triangle references tested (tri_fetch).  Other accelerators return MRT_ERR_STATE. */
 int mrt_trace_closest_counts(MrtScene *scene, const MrtRay *rays, uint32_t n, uint32_t *node_fetch,
                              uint32_t *tri_fetch, uint32_t mem);
 
@@ -285,14 +287,17 @@ int mrt_render(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *op
                uint32_t *bitmap, uint32_t stride_bytes, float *accum, uint32_t mem,
                MrtRenderStats *stats);
 /* mrt_render without any device allocation (no counterpart in the reference).  For callers that
- * cannot allocate device memory while rendering: code inside a CUDA stream capture, processes whose
- * device memory belongs to another allocator or a fixed budget, latency-critical threads.  bitmap
- * and accum are device pointers; all other scratch is one static device array of 12 MiB at most that
- * every GPU loading the library keeps until exit.  Supports the plain-rectangle block schedule only
- * (width a multiple of 16, stride_bytes = 4 * width, height / (height / 16) == 16), samplesLight <= 4
- * and depth_max <= 10; anything larger returns MRT_ERR_ARG.  The first call on a device looks up the
- * array's address (make it before any stream capture).  Calls share the array: calls that overlap
- * on the GPU race. */
+ * cannot allocate device memory while rendering: processes whose device memory belongs to another
+ * allocator or to a fixed budget (an engine that hands the renderer a pool and forbids cudaMalloc),
+ * and latency-critical threads that must not meet cudaMalloc / cudaFree's implicit device
+ * synchronisation.  bitmap and accum are device pointers; all other scratch is one static device
+ * array of 12 MiB at most that every GPU loading the library keeps until exit.  Supports the
+ * plain-rectangle block schedule only (width a multiple of 16, stride_bytes = 4 * width,
+ * height / (height / 16) == 16), samplesLight <= 4 and depth_max <= 10; anything larger returns
+ * MRT_ERR_ARG.  The call returns when its work on the context's stream has finished.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU (two host threads, or two
+ * contexts on one device) race.  mrt_render_stop and mrt_render_progress apply as for mrt_render. */
 int mrt_render_noalloc(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *opts, uint32_t *bitmap,
                        uint32_t stride_bytes, float *accum, MrtRenderStats *stats);
 void mrt_render_stop(MrtScene *scene);

@@ -3,7 +3,7 @@
 Used to feed mrt_trace_closest / mrt_trace_closest_counts with exactly the rays the render kernels
 generate (e.g. for the counting replay behind the roofline figure).  numpy float32 operations are
 IEEE binary32 with no fused multiply-add, so with the reference's operation order the rays equal the
-device ones bit for bit (checked against the oracle in tests/test_camera.py):
+device ones bit for bit (tests/test_camera.py compares them with the oracle's camera):
   Camera ctor (Camera.cpp:52-57), Perspective ctor and generateRay / fastArcTan
   (Perspective.cpp:10-44), Orthographic ctor and generateRay (Orthographic.cpp:12-34), pixel loop
   u = x / W, v = y / H (Renderer.cpp:94-104).

@@ -119,7 +119,9 @@ def reference_outputs():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MRT_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout>  (or set MRT_REFERENCE_DIR)")
     tt = open(os.path.join(ref, "app/Unit_Testing/TestTriangle.cpp")).read()
     tp = open(os.path.join(ref, "app/Unit_Testing/TestPlane.cpp")).read()
     cases = parse_triangle_tests(tt) + parse_plane_tests(tp)

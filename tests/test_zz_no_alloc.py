@@ -1,6 +1,6 @@
 """mrt_render_noalloc: the render entry point for callers that cannot allocate device memory while
-they render (code inside a CUDA stream capture, processes whose device memory belongs to another
-allocator or a fixed budget, latency-critical threads).  It keeps its scratch in one static device
+they render (processes whose device memory belongs to another allocator or a fixed budget,
+latency-critical threads that must not meet cudaMalloc's implicit synchronisation).  It keeps its scratch in one static device
 array instead of allocating, so it must produce exactly what mrt_render produces for the same device
 buffers, call after call (the array keeps the previous call's contents), and refuse requests
 beyond its fixed limits.  This file is collected last so a failure here comes after every other
@@ -27,6 +27,10 @@ CASES = [
     ("glass_room", capi.MRT_SHADER_WHITTED, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST, 2, 2),
     ("cornell_box", capi.MRT_SHADER_PATHTRACER, capi.MRT_ACCEL_BVH, capi.MRT_BVH_REFERENCE, 4, 1),
     ("soup", capi.MRT_SHADER_NOSHADOWS, capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST, 2, 1),
+    # the direct shaders on the accelerators without the persistent engine (one thread per pixel)
+    ("soup", capi.MRT_SHADER_NOSHADOWS, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST, 2, 1),
+    ("glass_room", capi.MRT_SHADER_DEPTHMAP, capi.MRT_ACCEL_BVH, capi.MRT_BVH_REFERENCE, 1, 1),
+    ("cornell_box", capi.MRT_SHADER_DIFFUSE, capi.MRT_ACCEL_NAIVE, capi.MRT_BVH_FAST, 1, 1),
 ]
 
 
