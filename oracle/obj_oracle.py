@@ -4,8 +4,10 @@ OBJLoader::process + OBJLoader::fillScene (app/Components/ObjectLoaders/OBJLoade
 tinyobjloader's LoadObj with triangulation on (OBJLoader.cpp:33-35).  tinyobjloader is an empty,
 unpinned submodule in the reference checkout, so neither it nor the loader can be compiled here:
 this file restates both from their published behaviour and from OBJLoader.cpp as read, independently
-of the library's C++ loader, and the tests compare the two.  Parity of this row is therefore pinned
-to the reference's source text, not to a run of the reference (parity unpinned).
+of the library's C++ loader, and the tests compare the two.  The conversion step is also pinned to
+the reference's own code: parse() feeds OBJLoader::fillScene, compiled from the reference sources
+(oracle/ref_driver.cpp, ref_obj_fill), and the tests compare its Scene with the library's loader.
+Only the parsing (tinyobjloader's, absent and unpinned) remains a restatement.
 
 Float32 arithmetic with numpy follows the reference's operation order (glm: normalize =
 v * (1 / sqrt(dot)), dot = (x*x + y*y) + z*z, cross as in the GLSL definition).
@@ -69,9 +71,9 @@ def _index(tok: str, n: int) -> int:
     return i - 1 if i > 0 else n + i
 
 
-def load(obj_path, mtl_path=None):
-    """(tri_abc, tri_normals, tri_colors, tri_material, materials, lights) as the reference builds
-    the Scene; materials as (Kd, Ks, Kt, ior, Le) tuples, lights as (A, B, C, material)."""
+def parse(obj_path, mtl_path=None):
+    """tinyobjloader's LoadObj with triangulation, restated: (positions, vertex colours, normals,
+    triangles as ((v, n), (v, n), (v, n), material), materials from read_mtl)."""
     mats, names = read_mtl(mtl_path) if mtl_path else ([], {})
     pos, col, nrm, tris = [], [], [], []
     cur = -1
@@ -97,6 +99,13 @@ def load(obj_path, mtl_path=None):
                 face.append((vi, ni))
             for k in range(1, len(face) - 1):   # tinyobj triangulation: a fan from the first vertex
                 tris.append((face[0], face[k], face[k + 1], cur))
+    return pos, col, nrm, tris, mats
+
+
+def load(obj_path, mtl_path=None):
+    """(tri_abc, tri_normals, tri_colors, tri_material, materials, lights) as the reference builds
+    the Scene; materials as (Kd, Ks, Kt, ior, Le) tuples, lights as (A, B, C, material)."""
+    pos, col, nrm, tris, mats = parse(obj_path, mtl_path)
     abc, normals, colors, tmat, materials, lights = [], [], [], [], [], []
     for a, b, c, m in tris:
         p = [np.array([-pos[v][0], pos[v][1], pos[v][2]], F) for v, _ in (a, b, c)]

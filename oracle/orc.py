@@ -99,6 +99,8 @@ def ref(fast: bool = False) -> ctypes.CDLL:
             "ref_trace_any": (ip, [vp, vp, vp, ctypes.c_uint32, vp, ip]),
             "ref_render": (ip, [vp, vp, vp, ip, ip, vp, ctypes.c_uint32, dp, dp]),
             "ref_render_subset": (ctypes.c_uint64, [vp, vp, vp, ip, ip, ctypes.c_uint32, ctypes.c_uint32, vp, dp, dp]),
+            "ref_obj_fill": (ip, [ctypes.c_char_p, ctypes.c_char_p, vp, vp, ctypes.c_uint32, vp, ctypes.c_uint32, vp,
+                                  vp, ctypes.c_uint32, vp, ctypes.c_uint32, vp, vp, vp, vp]),
         })
         _ref[key] = lib
     return _ref[key]
@@ -249,3 +251,33 @@ def ref_render_subset(scene, camera, opts, accel: int, threads: int, first: int,
     n = lib.ref_render_subset(ctypes.byref(desc), ctypes.byref(camera), ctypes.byref(opts), accel, threads, first,
                               step, bm.ctypes.data, ctypes.byref(tb), ctypes.byref(tr))
     return bm, int(n), tb.value, tr.value
+
+
+def ref_obj_fill(obj_path: str, mtl_path: str | None, parsed):
+    """OBJLoader::process + fillScene compiled from the reference sources, run on a staged parse
+    (obj_oracle.parse's result).  Returns (triangles (n, 30) float32 with A, AB, AC, normals,
+    colours and the material index as int bits in column 27, materials (m, 13) Le Kd Ks Kt ior,
+    area lights (k, 22) A AB AC + material)."""
+    pos, col, nrm, tris, mats = parsed
+    lib = ref()
+    v = np.ascontiguousarray(np.asarray(pos, np.float32).reshape(-1, 3))
+    c = np.ascontiguousarray(np.asarray(col, np.float32).reshape(-1, 3))
+    n = np.ascontiguousarray(np.asarray(nrm, np.float32).reshape(-1, 3)) if nrm else np.zeros((0, 3), np.float32)
+    idx = np.ascontiguousarray(np.array([[a[0], a[1], b[0], b[1], cc[0], cc[1]] for a, b, cc, _ in tris],
+                                        np.int32).reshape(-1, 6))
+    fmat = np.ascontiguousarray(np.array([m for *_, m in tris], np.int32))
+    mt = np.zeros((max(1, len(mats)), 14), np.float32)
+    for k, m in enumerate(mats):
+        mt[k, 0:3], mt[k, 3:6], mt[k, 6:9], mt[k, 9:12] = m["Kd"], m["Ks"], m["Kt"], m["Ke"]
+        mt[k, 12], mt[k, 13] = m["Ni"], m["d"]
+    nf = len(tris)
+    out_tri = np.zeros((max(1, nf), 30), np.float32)
+    out_mat = np.zeros((max(1, len(mats)), 13), np.float32)
+    out_light = np.zeros((max(1, nf), 22), np.float32)
+    counts = np.zeros(3, np.uint32)
+    st = lib.ref_obj_fill(obj_path.encode(), mtl_path.encode() if mtl_path else None, v.ctypes.data, c.ctypes.data,
+                          len(v), n.ctypes.data, len(n), idx.ctypes.data, fmat.ctypes.data, nf, mt.ctypes.data,
+                          len(mats), out_tri.ctypes.data, out_mat.ctypes.data, out_light.ctypes.data, counts.ctypes.data)
+    if st != 0:
+        raise RuntimeError(f"ref_obj_fill failed: {st}")
+    return out_tri[:counts[0]], out_mat[:counts[1]], out_light[:counts[2]]

@@ -8,12 +8,15 @@
 //   * closest-hit ids / any-hit flags   Shader::rayTrace / Shader::shadowTrace (Shader.cpp:124-187)
 //                                       through the reference's own accelerators
 //   * whole frames                      Renderer::renderFrame (Renderer.cpp:31-116)
+//   * OBJ scenes                        OBJLoader::process + OBJLoader::fillScene (OBJLoader.cpp:21-248)
+//                                       on a parse staged by the caller (tinyobjloader is absent)
 // Scenes arrive in the mrt_cuda.h MrtSceneDesc layout so the same arrays feed the CUDA path.
 #include "../include/mrt_cuda.h"
 
 #include "Components/Cameras/Orthographic.hpp"
 #include "Components/Cameras/Perspective.hpp"
 #include "Components/Lights/AreaLight.hpp"
+#include "Components/ObjectLoaders/OBJLoader.hpp"
 #include "Components/Lights/PointLight.hpp"
 #include "Components/Samplers/Constant.hpp"
 #include "Components/Samplers/HaltonSeq.hpp"
@@ -232,6 +235,49 @@ std::unique_ptr<::MobileRT::Camera> make_camera(const MrtCamera &c) {
 
 }  // namespace
 
+namespace {
+
+// ---- the staged parse behind tinyobj::LoadObj (oracle/shim/tinyobjloader/tiny_obj_loader.h) ----------
+struct ObjStage {
+    bool staged = false;
+    ::tinyobj::attrib_t attrib;
+    std::vector<::tinyobj::shape_t> shapes;
+    std::vector<::tinyobj::material_t> materials;
+};
+ObjStage &obj_stage() {
+    thread_local ObjStage st;
+    return st;
+}
+
+// read access to AreaLight::triangle_ (private in the reference) through an explicit instantiation,
+// which may name private members: the checker compares the light's triangle as the reference built it
+template <typename Tag, typename Tag::type M>
+struct Expose {
+    friend typename Tag::type get(Tag) { return M; }
+};
+struct AreaLightTriangle {
+    typedef ::MobileRT::Triangle Components::AreaLight::*type;
+    friend type get(AreaLightTriangle);
+};
+template struct Expose<AreaLightTriangle, &Components::AreaLight::triangle_>;
+
+}  // namespace
+
+namespace tinyobj {
+bool LoadObj(attrib_t *attrib, std::vector<shape_t> *shapes, std::vector<material_t> *materials, std::string *,
+             std::string *err, std::istream *, MaterialReader *, bool) {
+    ObjStage &st = obj_stage();
+    if (!st.staged) {
+        if (err) *err = "no staged parse";
+        return false;
+    }
+    *attrib = st.attrib;
+    *shapes = st.shapes;
+    *materials = st.materials;
+    return true;
+}
+}  // namespace tinyobj
+
 extern "C" {
 
 int ref_abi_version(void) { return 1; }
@@ -439,6 +485,77 @@ uint64_t ref_render_subset(const MrtSceneDesc *desc, const MrtCamera *camera, co
     });
     if (t_render) *t_render = seconds_since(t1);
     return count;
+}
+
+/* ---- OBJ scenes -------------------------------------------------------------------------------- */
+// The reference's OBJLoader::process and OBJLoader::fillScene on a parse the caller stages (vertices
+// with colours, normals, triangulated faces with their material ids, materials): the loader's own
+// conversion code builds the Scene.  Outputs, per scene triangle 30 floats (A, AB, AC, normals A B C,
+// colours A B C, material index as int bits), per material 13 (Le, Kd, Ks, Kt, ior), per area light 22
+// (its triangle's A, AB, AC, then its material's 13).  counts: triangles, materials, lights.
+int ref_obj_fill(const char *obj_path, const char *mtl_path, const float *vertices, const float *colors, uint32_t nv,
+                 const float *normals, uint32_t nn, const int32_t *face_idx, const int32_t *face_mat, uint32_t n_faces,
+                 const float *mats, uint32_t n_mat, float *out_tri, float *out_mat, float *out_light, uint32_t *counts) {
+    ObjStage &st = obj_stage();
+    st = ObjStage{};
+    st.attrib.vertices.assign(vertices, vertices + 3ull * nv);
+    st.attrib.colors.assign(colors, colors + 3ull * nv);
+    if (nn) st.attrib.normals.assign(normals, normals + 3ull * nn);
+    ::tinyobj::shape_t shape;
+    shape.name = "staged";
+    for (uint32_t f = 0; f < n_faces; ++f) {
+        for (int k = 0; k < 3; ++k)
+            shape.mesh.indices.push_back(::tinyobj::index_t{face_idx[6 * f + 2 * k], face_idx[6 * f + 2 * k + 1], -1});
+        shape.mesh.num_face_vertices.push_back(3u);
+        shape.mesh.material_ids.push_back(face_mat[f]);
+    }
+    st.shapes.push_back(std::move(shape));
+    for (uint32_t m = 0; m < n_mat; ++m) {
+        const float *x = mats + 14ull * m;
+        ::tinyobj::material_t t{};
+        for (int k = 0; k < 3; ++k) {
+            t.diffuse[k] = x[k];
+            t.specular[k] = x[3 + k];
+            t.transmittance[k] = x[6 + k];
+            t.emission[k] = x[9 + k];
+        }
+        t.ior = x[12];
+        t.dissolve = x[13];
+        st.materials.push_back(t);
+    }
+    st.staged = true;
+    Scene scene{};
+    {
+        ::Components::OBJLoader loader{obj_path, mtl_path ? mtl_path : ""};
+        if (loader.process() < 0 || !loader.isProcessed()) return 1;
+        if (!loader.fillScene(&scene, [] { return std::make_unique<::Components::Constant>(0.5f); })) return 2;
+    }
+    st = ObjStage{};
+    auto put3 = [](float *o, const ::glm::vec3 &v) { o[0] = v[0]; o[1] = v[1]; o[2] = v[2]; };
+    auto put_mat = [&](float *o, const Material &m) {
+        put3(o, m.Le_); put3(o + 3, m.Kd_); put3(o + 6, m.Ks_); put3(o + 9, m.Kt_); o[12] = m.refractiveIndice_;
+    };
+    auto put_tri = [&](float *o, const Triangle &t) { put3(o, t.pointA_); put3(o + 3, t.AB_); put3(o + 6, t.AC_); };
+    for (size_t i = 0; i < scene.triangles_.size(); ++i) {
+        const Triangle &t = scene.triangles_[i];
+        float *o = out_tri + 30 * i;
+        put_tri(o, t);
+        put3(o + 9, t.normalA_); put3(o + 12, t.normalB_); put3(o + 15, t.normalC_);
+        put3(o + 18, t.colorA_); put3(o + 21, t.colorB_); put3(o + 24, t.colorC_);
+        std::memcpy(o + 27, &t.materialId_, 4);
+        o[28] = o[29] = 0.0f;
+    }
+    for (size_t i = 0; i < scene.materials_.size(); ++i) put_mat(out_mat + 13 * i, scene.materials_[i]);
+    for (size_t i = 0; i < scene.lights_.size(); ++i) {
+        const auto *al = dynamic_cast<const ::Components::AreaLight *>(scene.lights_[i].get());
+        if (!al) return 3;
+        put_tri(out_light + 22 * i, al->*get(AreaLightTriangle{}));
+        put_mat(out_light + 22 * i + 9, al->radiance_);
+    }
+    counts[0] = static_cast<uint32_t>(scene.triangles_.size());
+    counts[1] = static_cast<uint32_t>(scene.materials_.size());
+    counts[2] = static_cast<uint32_t>(scene.lights_.size());
+    return 0;
 }
 
 }  // extern "C"

@@ -70,3 +70,100 @@ def test_loader_errors(tmp_path):
     assert "face index" in str(e.value)
     s = scenes.load_obj(OBJ)       # no MTL: every face without material, no lights
     assert len(s.lights) == 0 and (s.tri_material == -1).all() and s.n_triangles == 10 + 3 + 3 + 2 + 1 + 1
+
+
+# ---- the conversion pinned to the reference's own OBJLoader::fillScene ----------------------------
+# OBJLoader::fillScene (OBJLoader.cpp:68-248), compiled from the reference sources, runs on the
+# oracle's restatement of tinyobjloader's parse (the library is an absent submodule); its Scene must
+# equal the library loader's output bit for bit.  A face vertex without a normal in a file that has
+# normals makes the reference read normals[-1] (OBJLoader.cpp:111-124, undefined behaviour), so these
+# fixtures give either every face vertex a normal or the file none.
+
+def _write_random_obj(path_obj, path_mtl, seed: int, with_normals: bool):
+    rng = np.random.default_rng(seed)
+    mtl = ["newmtl white", "Kd 0.73 0.73 0.73",
+           "newmtl white_close", "Kd 0.7300004 0.73 0.73",       # within Epsilon of white: merged
+           "newmtl white_far", "Kd 0.7300100 0.73 0.73",         # not merged
+           "newmtl mirror", "Kd 0 0 0", "Ks 1.7 1.6 1.5",
+           "newmtl glass", "Tf 0.9 0.8 0.7", "d 0.25", "Ni 1.45",
+           "newmtl frosted", "Kd 0.2 0.3 0.4", "Kt 0.8 0.8 0.8", "Tr 0.6", "Ni 1.2",
+           "newmtl lamp", "Ke 12 9 3",
+           "newmtl dim", "Ke 0.4 0.9 0.2",
+           "newmtl lamp_close", "Ke 12.000001 9 3"]
+    open(path_mtl, "w").write("\n".join(mtl) + "\n")
+    names = ["white", "white_close", "white_far", "mirror", "glass", "frosted", "lamp", "dim", "lamp_close",
+             "not_defined"]
+    lines = ["# generated fixture"]
+    nv = 0
+    nn = 0
+    for f in range(120):
+        if f % 7 == 0:
+            lines.append(f"usemtl {names[int(rng.integers(len(names)))]}")
+        k = int(rng.choice([3, 3, 3, 4, 5]))
+        for _ in range(k):
+            p = rng.uniform(-1, 1, 3)
+            if rng.random() < 0.5:
+                c = rng.uniform(0, 1, 3)
+                lines.append("v %.7g %.7g %.7g %.5g %.5g %.5g" % (*p, *c))
+            else:
+                lines.append("v %.7g %.7g %.7g" % tuple(p))
+            nv += 1
+            if with_normals:
+                q = rng.normal(size=3) * (1.0 if rng.random() < 0.9 else 0.0)   # some zero normals
+                lines.append("vn %.6g %.6g %.6g" % tuple(q))
+                nn += 1
+        toks = []
+        for j in range(k):
+            vi = nv - k + 1 + j
+            v = str(vi) if rng.random() < 0.5 else str(vi - nv - 1)      # absolute or relative
+            if with_normals:
+                ni = nn - k + 1 + j
+                toks.append(f"{v}//{ni}")
+            else:
+                toks.append(v)
+        lines.append("f " + " ".join(toks))
+    open(path_obj, "w").write("\n".join(lines) + "\n")
+
+
+def _check_against_reference_fill(obj, mtl):
+    import orc as O
+    parsed = obj_oracle.parse(obj, mtl)
+    tri, mats, lights = O.ref_obj_fill(obj, mtl, parsed)
+    s = scenes.load_obj(obj, mtl)
+    F = np.float32
+    n = s.n_triangles
+    assert len(tri) == n and len(mats) == len(s.materials) and len(lights) == len(s.lights)
+    A = s.tri_abc[:, 0:3]
+    want = np.concatenate([A, s.tri_abc[:, 3:6] - A, s.tri_abc[:, 6:9] - A, s.tri_normals, s.tri_colors], 1).astype(F)
+    assert np.array_equal(tri[:, :27].view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(tri[:, 27].view(np.int32), s.tri_material)
+    got_m = np.array([[*m.le, *m.kd, *m.ks, *m.kt, m.ior] for m in s.materials], F).reshape(-1, 13)
+    assert np.array_equal(mats.view(np.uint32), got_m.view(np.uint32))
+    got_l = np.array([[*l.p0, *(np.array(l.p1, F) - np.array(l.p0, F)), *(np.array(l.p2, F) - np.array(l.p0, F)),
+                       *l.radiance.le, *l.radiance.kd, *l.radiance.ks, *l.radiance.kt, l.radiance.ior]
+                      for l in s.lights], F).reshape(-1, 22)
+    assert np.array_equal(lights.view(np.uint32), got_l.view(np.uint32))
+    return n, len(mats), len(lights)
+
+
+def test_room_without_normals_equals_reference_fill_scene(tmp_path):
+    text = open(OBJ).read().splitlines()
+    kept = []
+    for line in text:
+        if line.startswith("vn "):
+            continue
+        if line.startswith("f "):
+            line = "f " + " ".join(t.split("/")[0] for t in line.split()[1:])
+        kept.append(line)
+    obj = str(tmp_path / "room_plain.obj")
+    open(obj, "w").write("\n".join(kept) + "\n")
+    n, m, l = _check_against_reference_fill(obj, MTL)
+    assert (n, l) == (17, 3) and m == 5
+
+
+@pytest.mark.parametrize("seed,with_normals", [(1, True), (2, False), (3, True)])
+def test_generated_scenes_equal_reference_fill_scene(tmp_path, seed, with_normals):
+    obj, mtl = str(tmp_path / "g.obj"), str(tmp_path / "g.mtl")
+    _write_random_obj(obj, mtl, seed, with_normals)
+    n, m, l = _check_against_reference_fill(obj, mtl)
+    assert n > 0 and l > 0 and m > 0
