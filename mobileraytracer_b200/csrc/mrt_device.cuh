@@ -280,9 +280,29 @@ MRT_HD float halton(uint32_t index, uint32_t base) {
     return result;
 }
 
-MRT_HD uint32_t prime16(uint32_t i) {
-    const uint32_t p[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
-    return p[i & 15u];
+// Halton base of sample dimension `dim`: the dim-th prime.  The dimensions in use are 0-1 (camera
+// jitter), 2 (roulette) and 8 + 3j + 1, 8 + 3j + 2 (position on the light of light sample j < 32),
+// all below kHaltonDims, so no two dimensions share a base.
+constexpr uint32_t kHaltonDims = 128;
+#define MRT_HALTON_PRIMES \
+    2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, \
+    59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127, 131, \
+    137, 139, 149, 151, 157, 163, 167, 173, 179, 181, 191, 193, 197, 199, 211, 223, \
+    227, 229, 233, 239, 241, 251, 257, 263, 269, 271, 277, 281, 283, 293, 307, 311, \
+    313, 317, 331, 337, 347, 349, 353, 359, 367, 373, 379, 383, 389, 397, 401, 409, \
+    419, 421, 431, 433, 439, 443, 449, 457, 461, 463, 467, 479, 487, 491, 499, 503, \
+    509, 521, 523, 541, 547, 557, 563, 569, 571, 577, 587, 593, 599, 601, 607, 613, \
+    617, 619, 631, 641, 643, 647, 653, 659, 661, 673, 677, 683, 691, 701, 709, 719
+#ifdef __CUDACC__
+static __constant__ uint32_t c_halton_primes[kHaltonDims] = {MRT_HALTON_PRIMES};
+#endif
+static const uint32_t h_halton_primes[kHaltonDims] = {MRT_HALTON_PRIMES};
+MRT_HD uint32_t halton_base(uint32_t dim) {
+#ifdef __CUDA_ARCH__
+    return c_halton_primes[dim % kHaltonDims];
+#else
+    return h_halton_primes[dim % kHaltonDims];
+#endif
 }
 
 struct Stream {
@@ -314,7 +334,7 @@ MRT_HD float draw(const Stream &st, int kind, uint32_t node, uint32_t dim) {
             return v;
         }
         case MRT_SAMPLER_HALTON: {
-            float v = halton(st.sample, prime16(dim)) + key_float(st.rot_base, node, dim);
+            float v = halton(st.sample, halton_base(dim)) + key_float(st.rot_base, node, dim);
             if (v >= 1.0f) v -= 1.0f;
             return v;
         }

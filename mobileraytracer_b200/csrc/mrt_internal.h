@@ -50,8 +50,8 @@ struct MrtContext {
     // render scratch shared by the context's scenes (renders on one context are serialised on its
     // stream): wavefront queues, per-sample values, host-path bitmap staging
     DevBuf wave[8];
-    // raster preview scratch: depth keys, queued large triangles, counters, host-path bitmap
-    DevBuf raster[4];
+    // raster preview scratch: depth keys, queued large triangles, counters, host-path bitmap, overflow lists
+    DevBuf raster[5];
 };
 
 struct RefBvhHost {

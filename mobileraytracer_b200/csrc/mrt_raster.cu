@@ -42,7 +42,10 @@ namespace {
 constexpr float kSub = 256.0f;            // snapped window coordinates: 1/256 pixel
 constexpr float kGuard = 16.0f;           // x, y clipped to +-16 w
 constexpr uint32_t kSmallPixels = 64;     // bounding boxes up to this many pixels: one thread
-constexpr int kMaxPoly = 9;               // a triangle clipped by six planes
+// a triangle clipped by six planes has at most 9 vertices in exact arithmetic; rounded intersection
+// points can make the polygon slightly non-convex and let a later plane add more, so the clipper
+// keeps room for 16 and drops any vertex beyond that (the oracle does the same)
+constexpr int kMaxPoly = 16;
 constexpr uint32_t kMaxSide = 8192;       // frame sides (keeps every snapped coordinate in 32 bits)
 
 // column-major 4x4: element (row r, column c) at m[4 c + r], as android.opengl.Matrix
@@ -150,8 +153,11 @@ struct RasterParams {
     unsigned long long *keys;     // width x height: (depth bits << 32) | (0xFFFFFFFF - triangle)
     RasterTri *big;
     uint32_t big_cap;
-    unsigned long long *counts;   // [0] queued, [1] drawn, [2] fragments
+    unsigned long long *counts;   // [0] queued, [1] drawn, [2] fragments, [3] triangles sent to the next pass
+    uint32_t *overflow;           // triangles whose large pieces found the queue full
 };
+
+constexpr uint32_t kEmptyQueued = 0xFFFFFFFFu;   // a queue slot left empty by a triangle sent to the next pass
 
 struct Clip {
     float x, y, z, w;
@@ -257,17 +263,25 @@ __device__ __forceinline__ Win to_window(const RasterParams &p, const Clip &c) {
     return Win{__float2int_rn((hw * xn + hw) * kSub), __float2int_rn((hh * yn + hh) * kSub), 0.5f * zn + 0.5f};
 }
 
-// one triangle in window coordinates: back faces and empty boxes dropped, large boxes queued for
-// k_raster_big, small ones covered here
-__device__ __forceinline__ void draw_triangle(const RasterParams &p, uint32_t tri, Win a, Win b, Win c,
-                                              unsigned long long &drawn, unsigned long long &frags) {
+// one triangle in window coordinates: back faces and empty boxes dropped (kind 0), boxes of up to
+// kSmallPixels pixels covered here (kind 1), larger ones queued for k_raster_big (kind 2), front
+// faces whose box misses the viewport counted as drawn only (kind 3)
+struct SubTri {
     Setup t;
+    int kind;
+    uint32_t x0, x1, y0, y1;
+};
+
+__device__ __forceinline__ SubTri setup_sub(const RasterParams &p, Win a, Win b, Win c) {
+    SubTri u;
+    Setup &t = u.t;
+    u.kind = 0;
+    u.x0 = u.x1 = u.y0 = u.y1 = 0;
     t.x[0] = a.x; t.y[0] = a.y; t.z[0] = a.z;
     t.x[1] = b.x; t.y[1] = b.y; t.z[1] = b.z;
     t.x[2] = c.x; t.y[2] = c.y; t.z[2] = c.z;
     t.area2 = edge_fn(t.x[0], t.y[0], t.x[1], t.y[1], t.x[2], t.y[2]);
-    if (t.area2 <= 0) return;   // clockwise (back face, culled) or no area
-    ++drawn;
+    if (t.area2 <= 0) return u;   // clockwise (back face, culled) or no area
     t.tl12 = top_left(t.x[1], t.y[1], t.x[2], t.y[2]);
     t.tl20 = top_left(t.x[2], t.y[2], t.x[0], t.y[0]);
     t.tl01 = top_left(t.x[0], t.y[0], t.x[1], t.y[1]);
@@ -278,20 +292,41 @@ __device__ __forceinline__ void draw_triangle(const RasterParams &p, uint32_t tr
     const long long bx1 = min((long long)p.width - 1, floor_div256(xmax - 128));
     const long long by0 = max(0ll, -floor_div256(-(ymin - 128)));
     const long long by1 = min((long long)p.height - 1, floor_div256(ymax - 128));
-    if (bx0 > bx1 || by0 > by1) return;
+    if (bx0 > bx1 || by0 > by1) { u.kind = 3; return u; }   // drawn, nothing covered
+    u.x0 = (uint32_t)bx0; u.x1 = (uint32_t)bx1; u.y0 = (uint32_t)by0; u.y1 = (uint32_t)by1;
     const uint64_t box = (uint64_t)(bx1 - bx0 + 1) * (uint64_t)(by1 - by0 + 1);
-    if (box > kSmallPixels) {
-        const unsigned long long q = atomicAdd(&p.counts[0], 1ull);
-        if (q < p.big_cap) {
-            RasterTri r;
-            for (int j = 0; j < 3; ++j) { r.x[j] = t.x[j]; r.y[j] = t.y[j]; r.z[j] = t.z[j]; }
-            r.tri = tri;
-            r.x0 = (uint32_t)bx0; r.x1 = (uint32_t)bx1; r.y0 = (uint32_t)by0; r.y1 = (uint32_t)by1;
-            p.big[q] = r;
-            return;
-        }
+    u.kind = box > kSmallPixels ? 2 : 1;
+    return u;
+}
+
+__device__ __forceinline__ void draw_sub(const RasterParams &p, uint32_t tri, const SubTri &u, uint32_t &qslot,
+                                         unsigned long long &drawn, unsigned long long &frags) {
+    if (u.kind == 0) return;
+    ++drawn;
+    if (u.kind == 3) return;
+    if (u.kind == 2) {
+        RasterTri r;
+        for (int j = 0; j < 3; ++j) { r.x[j] = u.t.x[j]; r.y[j] = u.t.y[j]; r.z[j] = u.t.z[j]; }
+        r.tri = tri;
+        r.x0 = u.x0; r.x1 = u.x1; r.y0 = u.y0; r.y1 = u.y1;
+        p.big[qslot++] = r;
+        return;
     }
-    frags += cover_box(p, t, tri, (uint32_t)bx0, (uint32_t)bx1, (uint32_t)by0, (uint32_t)by1);
+    frags += cover_box(p, u.t, tri, u.x0, u.x1, u.y0, u.y1);
+}
+
+// Queue slots for a triangle's `nbig` large pieces, all or none.  When the queue has no room the
+// triangle goes whole to the overflow list (drawn by a later pass, which keeps the result: the depth
+// test is an atomicMin of (depth, triangle) keys, the same in any order); slots it was handed below
+// the queue's end are marked empty for k_raster_big.
+__device__ __forceinline__ bool reserve(const RasterParams &p, uint32_t tri, uint32_t nbig, uint32_t &qslot) {
+    if (nbig == 0) return true;
+    const unsigned long long q = atomicAdd(&p.counts[0], (unsigned long long)nbig);
+    if (q + nbig <= p.big_cap) { qslot = (uint32_t)q; return true; }
+    for (unsigned long long k = q; k < p.big_cap; ++k) p.big[k].tri = kEmptyQueued;
+    const unsigned long long o = atomicAdd(&p.counts[3], 1ull);
+    p.overflow[o] = tri;   // o < triangles of this pass: each triangle is sent on at most once
+    return false;
 }
 
 // a triangle that leaves the near/far planes or the guard band: Sutherland-Hodgman against the six
@@ -307,8 +342,8 @@ __device__ __noinline__ void draw_clipped(const RasterParams &p, uint32_t tri, C
         for (int k = 0; k < n; ++k) {
             const Clip S = poly[k], E = poly[k + 1 < n ? k + 1 : 0];
             const float ds = plane_dist(S, q), de = plane_dist(E, q);
-            if (ds >= 0.0f) tmp[m++] = S;
-            if ((ds >= 0.0f) != (de >= 0.0f)) {
+            if (ds >= 0.0f && m < kMaxPoly) tmp[m++] = S;
+            if ((ds >= 0.0f) != (de >= 0.0f) && m < kMaxPoly) {
                 const float t = ds / (ds - de);
                 tmp[m++] = Clip{S.x + t * (E.x - S.x), S.y + t * (E.y - S.y), S.z + t * (E.z - S.z), S.w + t * (E.w - S.w)};
             }
@@ -319,14 +354,20 @@ __device__ __noinline__ void draw_clipped(const RasterParams &p, uint32_t tri, C
     if (n < 3) return;
     Win w[kMaxPoly];
     for (int k = 0; k < n; ++k) w[k] = to_window(p, poly[k]);
-    for (int k = 1; k + 1 < n; ++k) draw_triangle(p, tri, w[0], w[k], w[k + 1], drawn, frags);
+    uint32_t nbig = 0;
+    for (int k = 1; k + 1 < n; ++k) nbig += setup_sub(p, w[0], w[k], w[k + 1]).kind == 2 ? 1u : 0u;
+    uint32_t qslot = 0;
+    if (!reserve(p, tri, nbig, qslot)) return;
+    for (int k = 1; k + 1 < n; ++k) draw_sub(p, tri, setup_sub(p, w[0], w[k], w[k + 1]), qslot, drawn, frags);
 }
 
-__global__ void __launch_bounds__(128, 8) k_raster_tris(DevScene s, RasterParams p) {
+// one thread per triangle of the pass: all scene triangles, or the overflow list of the last pass
+__global__ void __launch_bounds__(128, 8) k_raster_tris(DevScene s, RasterParams p, const uint32_t *list, uint32_t n_items) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long drawn = 0, frags = 0;
-    if (i < s.n_tri) {
-        const float4 a = s.tri_a[i], ab = s.tri_ab[i], ac = s.tri_ac[i];
+    if (i < n_items) {
+        const uint32_t tri = list ? list[i] : i;
+        const float4 a = s.tri_a[tri], ab = s.tri_ab[tri], ac = s.tri_ac[tri];
         // DrawView.cpp:131-154: A, A + AB, A + AC, z negated
         const Clip c0 = to_clip(p.m, a.x, a.y, -a.z);
         const Clip c1 = to_clip(p.m, a.x + ab.x, a.y + ab.y, -(a.z + ab.z));
@@ -334,8 +375,13 @@ __global__ void __launch_bounds__(128, 8) k_raster_tris(DevScene s, RasterParams
         bool inside = true;
         for (int q = 0; q < 6; ++q)
             inside = inside && plane_dist(c0, q) >= 0.0f && plane_dist(c1, q) >= 0.0f && plane_dist(c2, q) >= 0.0f;
-        if (inside) draw_triangle(p, i, to_window(p, c0), to_window(p, c1), to_window(p, c2), drawn, frags);
-        else draw_clipped(p, i, c0, c1, c2, drawn, frags);
+        if (inside) {
+            const SubTri u = setup_sub(p, to_window(p, c0), to_window(p, c1), to_window(p, c2));
+            uint32_t qslot = 0;
+            if (reserve(p, tri, u.kind == 2 ? 1u : 0u, qslot)) draw_sub(p, tri, u, qslot, drawn, frags);
+        } else {
+            draw_clipped(p, tri, c0, c1, c2, drawn, frags);
+        }
     }
     drawn = warp_sum(drawn);
     frags = warp_sum(frags);
@@ -351,6 +397,7 @@ __global__ void __launch_bounds__(256) k_raster_big(RasterParams p) {
     unsigned long long frags = 0;
     for (uint32_t b = blockIdx.x; b < n; b += gridDim.x) {
         const RasterTri r = p.big[b];
+        if (r.tri == kEmptyQueued) continue;
         Setup t;
         for (int j = 0; j < 3; ++j) { t.x[j] = r.x[j]; t.y[j] = r.y[j]; t.z[j] = r.z[j]; }
         t.area2 = edge_fn(t.x[0], t.y[0], t.x[1], t.y[1], t.x[2], t.y[2]);
@@ -427,12 +474,20 @@ extern "C" int mrt_raster_preview(MrtScene *s, const MrtCamera *cam, uint32_t wi
     cudaSetDevice(ctx->device);
     cudaStream_t q = ctx->stream;
     const size_t pixels = (size_t)width * height;
-    // queue room for every triangle of scenes up to 2^20 triangles (58 MB); beyond that, large
-    // triangles that find the queue full are covered by their own thread (same result, slower)
-    const uint32_t big_cap = std::min<uint32_t>(s->n_tri, 1u << 20) + 1024u;
+    // queue room for every triangle of scenes up to 2^20 triangles (58 MB); beyond that, triangles
+    // whose large pieces find the queue full are drawn by further passes over an overflow list (same
+    // result).  MRT_RASTER_QUEUE_CAP lowers the room (tests force the further passes with it); it
+    // stays at least kMaxPoly - 2, the pieces of one clipped triangle, so every pass draws something.
+    uint32_t big_cap = std::min<uint32_t>(s->n_tri, 1u << 20) + 1024u;
+    if (const char *e = getenv("MRT_RASTER_QUEUE_CAP")) {
+        const long v = atol(e);
+        if (v > 0 && (unsigned long)v < big_cap) big_cap = (uint32_t)v;
+    }
+    big_cap = std::max<uint32_t>(big_cap, (uint32_t)(kMaxPoly - 2));
     int st = ensure(ctx, ctx->raster[0], 8 * pixels);
     if (st == MRT_OK) st = ensure(ctx, ctx->raster[1], sizeof(RasterTri) * (size_t)big_cap);
     if (st == MRT_OK) st = ensure(ctx, ctx->raster[2], 4 * sizeof(unsigned long long));
+    if (st == MRT_OK) st = ensure(ctx, ctx->raster[4], 2 * sizeof(uint32_t) * (size_t)std::max<uint32_t>(s->n_tri, 1u));
     const size_t bm_bytes = (size_t)stride_bytes * height;
     uint32_t *d_bitmap = bitmap;
     if (st == MRT_OK && mem == MRT_MEM_HOST) {
@@ -452,20 +507,40 @@ extern "C" int mrt_raster_preview(MrtScene *s, const MrtCamera *cam, uint32_t wi
     p.big = (RasterTri *)ctx->raster[1].ptr;
     p.big_cap = big_cap;
     p.counts = (unsigned long long *)ctx->raster[2].ptr;
+    uint32_t *lists[2] = {(uint32_t *)ctx->raster[4].ptr, (uint32_t *)ctx->raster[4].ptr + std::max<uint32_t>(s->n_tri, 1u)};
+    p.overflow = lists[0];
+    const int grid = (int)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 32);
     cudaEventRecord(ctx->ev0, q);
     cudaMemsetAsync(p.keys, 0xFF, 8 * pixels, q);
     cudaMemsetAsync(p.counts, 0, 4 * sizeof(unsigned long long), q);
     if (s->n_tri > 0) {
-        k_raster_tris<<<(s->n_tri + 127) / 128, 128, 0, q>>>(s->dev, p);
+        k_raster_tris<<<(s->n_tri + 127) / 128, 128, 0, q>>>(s->dev, p, nullptr, s->n_tri);
         k_raster_big<<<ctx->sm_count * 8, 256, 0, q>>>(p);
     }
-    const int grid = (int)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 32);
     k_raster_resolve<<<grid, 256, 0, q>>>(s->dev, p, d_bitmap, stride_bytes / 4u);
     cudaEventRecord(ctx->ev1, q);
     st = cuda_status(ctx, cudaGetLastError(), "raster kernels");
     unsigned long long counts[4] = {0, 0, 0, 0};
     if (st == MRT_OK)
         st = cuda_status(ctx, cudaMemcpyAsync(counts, p.counts, sizeof(counts), cudaMemcpyDeviceToHost, q), "raster counts");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "raster preview");
+    // triangles sent on by a full queue: further passes over the overflow list (only scenes whose
+    // large pieces exceed the queue), the image resolved again after each
+    for (int pass = 1; st == MRT_OK && counts[3] > 0; ++pass) {
+        if ((uint64_t)pass > (uint64_t)s->n_tri + 1) { set_error(ctx, "mrt_raster_preview: no progress"); return MRT_ERR_LIMIT; }
+        const uint32_t n_items = (uint32_t)counts[3];
+        const uint32_t *in = p.overflow;
+        p.overflow = in == lists[0] ? lists[1] : lists[0];
+        cudaMemsetAsync(p.counts, 0, sizeof(unsigned long long), q);
+        cudaMemsetAsync(p.counts + 3, 0, sizeof(unsigned long long), q);
+        k_raster_tris<<<(n_items + 127) / 128, 128, 0, q>>>(s->dev, p, in, n_items);
+        k_raster_big<<<ctx->sm_count * 8, 256, 0, q>>>(p);
+        k_raster_resolve<<<grid, 256, 0, q>>>(s->dev, p, d_bitmap, stride_bytes / 4u);
+        st = cuda_status(ctx, cudaGetLastError(), "raster kernels");
+        if (st == MRT_OK)
+            st = cuda_status(ctx, cudaMemcpyAsync(counts, p.counts, sizeof(counts), cudaMemcpyDeviceToHost, q), "raster counts");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "raster preview");
+    }
     if (st == MRT_OK && mem == MRT_MEM_HOST)
         st = cuda_status(ctx, cudaMemcpyAsync(bitmap, d_bitmap, bm_bytes, cudaMemcpyDeviceToHost, q), "bitmap out");
     if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "raster preview");

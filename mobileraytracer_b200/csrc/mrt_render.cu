@@ -769,20 +769,22 @@ uint32_t mrt_render_progress(const MrtScene *s) { return s ? s->progress.load() 
 // =============================================================================================
 // mrt_render_noalloc: the same render with every piece of scratch in a fixed device array.
 //
-// For callers that cannot allocate device memory while they render: code running inside a
-// cudaStreamBeginCapture region (an allocation there would break the capture), a process whose
-// device memory is owned by another allocator or a fixed budget, or a latency-critical thread that
-// must not hit cudaMalloc's implicit synchronisation.  The caller passes device buffers for the
-// bitmap and the sums; everything else the kernels need (work counters, the wave's ray / node /
-// shadow queues, per-sample values) lives in g_noalloc_scratch below, which every GPU that loads
-// the library holds until the process exits.
+// For callers that cannot allocate device memory while they render: a process whose device memory
+// is owned by another allocator or a fixed budget (an engine that lends the renderer a pool and
+// forbids cudaMalloc), or a latency-critical thread that must not hit cudaMalloc / cudaFree's implicit
+// synchronisation.  The caller passes device buffers for the bitmap and the sums; everything else the
+// kernels need (work counters, the wave's ray / node / shadow queues, per-sample values) lives in
+// g_noalloc_scratch below, which every GPU that loads the library holds until the process exits.
 //
 // Limits of this variant: image sizes whose block schedule is the plain rectangle (width a multiple
 // of 16, row pitch = width, as the reference CLI sizes images), samplesLight <= kNoAllocMaxSpl,
 // depth_max <= kNoAllocMaxDepth; waves of kNoAllocWave camera paths.  Larger requests fail with
-// MRT_ERR_ARG.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
-// array: calls that overlap on the GPU (two host threads, or two contexts on one device) race.
+// MRT_ERR_ARG.  The call returns once its work on the context's stream has finished (it waits on
+// events and on the stream, as mrt_render does).  The first call on a device looks up the array's
+// device address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls
+// share the array: calls that overlap on the GPU (two host threads, or two contexts on one device)
+// race.  As in mrt_render, at most one wave is queued ahead of the running one, so mrt_render_stop
+// ends the render within two waves and mrt_render_progress counts finished waves.
 // =============================================================================================
 namespace {
 
@@ -902,7 +904,15 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
         cudaMemsetAsync(w.counters, 0, 16, q);
         const uint64_t total_roots = (uint64_t)p.n_tasks * o->spp;
         p.task_base = 0;
+        uint64_t waves_issued = 0;
+        uint64_t done_samples[2] = {0, 0};
         for (uint64_t r0 = 0; r0 < total_roots; r0 += kNoAllocWave) {
+            if (waves_issued >= 2) {   // at most one wave queued ahead of the running one
+                const int slot = (int)(waves_issued % 2);
+                st = cuda_status(ctx, cudaEventSynchronize(ctx->wave_ev[slot]), "render");
+                if (st != MRT_OK) return st;
+                s->progress.store((uint32_t)done_samples[slot]);
+            }
             if (s->stop.load()) return cancelled(ctx, q);
             w.root_first = (uint32_t)r0;
             w.n_roots = (uint32_t)std::min<uint64_t>(kNoAllocWave, total_roots - r0);
@@ -912,6 +922,10 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
             for (int b = 0; b < levels; ++b) MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, counters);
             for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
             k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
+            const int slot = (int)(waves_issued % 2);
+            cudaEventRecord(ctx->wave_ev[slot], q);
+            done_samples[slot] = (r0 + w.n_roots) / std::max<uint64_t>(1, p.n_tasks);
+            ++waves_issued;
         }
         unsigned long long cnt[2] = {0, 0};
         st = cuda_status(ctx, cudaMemcpyAsync(cnt, w.counters, 16, cudaMemcpyDeviceToHost, q), "counters");

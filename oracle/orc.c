@@ -1037,7 +1037,19 @@ static inline float key_float(uint32_t base, uint32_t node, uint32_t dim) {
     const uint32_t h = mix32(mix32(base ^ node) ^ dim);
     return (float)(h >> 8) * (1.0f / 16777216.0f);
 }
-static const uint32_t PRIMES[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+/* Halton base of dimension dim: the dim-th prime (dims 0-1 camera, 2 roulette, 8 + 3j + 1..2 light
+ * sample j < 32 all lie below 128, so no two dimensions share a base) */
+#define HALTON_DIMS 128u
+static const uint32_t PRIMES[HALTON_DIMS] = {
+    2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
+    59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127, 131,
+    137, 139, 149, 151, 157, 163, 167, 173, 179, 181, 191, 193, 197, 199, 211, 223,
+    227, 229, 233, 239, 241, 251, 257, 263, 269, 271, 277, 281, 283, 293, 307, 311,
+    313, 317, 331, 337, 347, 349, 353, 359, 367, 373, 379, 383, 389, 397, 401, 409,
+    419, 421, 431, 433, 439, 443, 449, 457, 461, 463, 467, 479, 487, 491, 499, 503,
+    509, 521, 523, 541, 547, 557, 563, 569, 571, 577, 587, 593, 599, 601, 607, 613,
+    617, 619, 631, 641, 643, 647, 653, 659, 661, 673, 677, 683, 691, 701, 709, 719,
+};
 
 /* haltonSequence  Utils.cpp:36-45 */
 float orc_halton(uint32_t index, uint32_t base) {
@@ -1067,7 +1079,7 @@ static float stream_draw(const Stream *st, int kind, uint32_t node, uint32_t dim
             return v;
         }
         case MRT_SAMPLER_HALTON: {
-            float v = orc_halton(st->sample, PRIMES[dim & 15u]) + key_float(st->rot_base, node, dim);
+            float v = orc_halton(st->sample, PRIMES[dim % HALTON_DIMS]) + key_float(st->rot_base, node, dim);
             if (v >= 1.0f) v -= 1.0f;
             return v;
         }
@@ -1592,6 +1604,9 @@ int orc_aabb_intersect(const float *bmin, const float *bmax, const float *o, con
  * pixel, pixel centres with the top-left rule, linear window-space depth clamped to [0, 1]); this is
  * an independent serial restatement with a literal LEQUAL depth buffer in draw order. */
 typedef struct { float m[16]; } M4;   /* column-major: (row r, column c) at m[4 c + r] */
+/* clipped polygon: at most 9 vertices in exact arithmetic; rounding can make it slightly non-convex
+ * and let a later plane add more, so there is room for 16 and vertices beyond that are dropped */
+#define RAS_MAX_POLY 16
 typedef struct { float x, y, z, w; } C4;
 
 static M4 m4_perspective(float fovy, float aspect, float zn, float zf) {
@@ -1692,7 +1707,7 @@ int orc_raster_preview(const MrtSceneDesc *d, const MrtCamera *cam, uint32_t wid
     for (uint32_t i = 0; i < d->n_triangles; ++i) {
         const float *t = d->tri_abc + 9 * (size_t)i;
         const V3 A = vld(t), AB = vsub(vld(t + 3), A), AC = vsub(vld(t + 6), A);   /* Triangle.cpp: AB, AC */
-        C4 poly[9], tmp[9];
+        C4 poly[RAS_MAX_POLY], tmp[RAS_MAX_POLY];
         poly[0] = ras_clip(&m, v3(A.x, A.y, -A.z));
         poly[1] = ras_clip(&m, v3(A.x + AB.x, A.y + AB.y, -(A.z + AB.z)));
         poly[2] = ras_clip(&m, v3(A.x + AC.x, A.y + AC.y, -(A.z + AC.z)));
@@ -1702,8 +1717,8 @@ int orc_raster_preview(const MrtSceneDesc *d, const MrtCamera *cam, uint32_t wid
             for (int q = 0; q < n; ++q) {
                 const C4 S = poly[q], E = poly[(q + 1) % n];
                 const float ds = ras_plane(S, p), de = ras_plane(E, p);
-                if (ds >= 0.0f) tmp[out++] = S;
-                if ((ds >= 0.0f) != (de >= 0.0f)) {
+                if (ds >= 0.0f && out < RAS_MAX_POLY) tmp[out++] = S;
+                if ((ds >= 0.0f) != (de >= 0.0f) && out < RAS_MAX_POLY) {
                     const float u = ds / (ds - de);
                     C4 c; c.x = S.x + u * (E.x - S.x); c.y = S.y + u * (E.y - S.y); c.z = S.z + u * (E.z - S.z);
                     c.w = S.w + u * (E.w - S.w);
@@ -1714,8 +1729,8 @@ int orc_raster_preview(const MrtSceneDesc *d, const MrtCamera *cam, uint32_t wid
             memcpy(poly, tmp, sizeof(C4) * (size_t)n);
         }
         if (n < 3) continue;
-        int64_t X[9], Y[9];
-        float Z[9];
+        int64_t X[RAS_MAX_POLY], Y[RAS_MAX_POLY];
+        float Z[RAS_MAX_POLY];
         for (int q = 0; q < n; ++q) {
             const float xn = poly[q].x / poly[q].w, yn = poly[q].y / poly[q].w, zn = poly[q].z / poly[q].w;
             X[q] = (int64_t)lrintf((hw * xn + hw) * 256.0f);
