@@ -589,8 +589,9 @@ int mrt_trace_closest_counts(MrtScene *s, const MrtRay *rays, uint32_t n, uint32
         misaligned(ctx, mem, tri_fetch, 4, "tri_fetch"))
         return MRT_ERR_ARG;
     if (!s->built) { set_error(ctx, "mrt_trace_closest_counts before mrt_scene_build"); return MRT_ERR_STATE; }
-    if (s->opts.accelerator != MRT_ACCEL_BVH || s->opts.bvh_mode != MRT_BVH_FAST) {
-        set_error(ctx, "mrt_trace_closest_counts: only the FAST BVH has a counting replay");
+    if (!(s->opts.accelerator == MRT_ACCEL_BVH && s->opts.bvh_mode == MRT_BVH_FAST) &&
+        s->opts.accelerator != MRT_ACCEL_REGULAR_GRID) {
+        set_error(ctx, "mrt_trace_closest_counts: only the FAST BVH and the regular grid have a counting replay");
         return MRT_ERR_STATE;
     }
     if (n == 0) return MRT_OK;

@@ -1,8 +1,8 @@
 // mrt_kernels.cu - batch traversal kernels behind mrt_trace_closest / mrt_trace_any /
 // mrt_trace_closest_counts.  One thread per ray; rays are 32-byte MrtRay records read as two
 // 128-bit loads.
+#include "mrt_gridwalk.cuh"
 #include "mrt_internal.h"
-#include "mrt_persistent.cuh"
 
 using namespace mrt;
 using namespace mrt_host;
@@ -109,6 +109,28 @@ __global__ void __launch_bounds__(128, 8) k_trace_persistent(DevScene s, TraceWo
     persistent_closest<kCount>(s, work, lane);
 }
 
+__global__ void __launch_bounds__(128, 8) k_trace_grid_persistent(DevScene s, TraceWork<false> work) {
+    TraceLane lane;
+    persistent_grid_closest(s, work, lane);
+}
+
+// counting replay of the grid closest hit: planes and spheres in order, then the triangle grid
+// (counted: cells visited and triangle references tested), as k_trace_closest
+__global__ void __launch_bounds__(128) k_trace_counts_grid(DevScene s, const MrtRay *rays, uint32_t n, uint32_t *cells,
+                                                           uint32_t *refs) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Ray r = load_ray(rays, i);
+        float len = kRayLengthMax;
+        uint32_t id = MRT_HIT_NONE;
+        grid_trace<kPlane>(s, r, len, id);
+        grid_trace<kSphere>(s, r, len, id);
+        GridCounts c{0, 0};
+        grid_trace<kTriangle, true>(s, r, len, id, &c);
+        cells[i] = c.cells;
+        refs[i] = c.refs;
+    }
+}
+
 template <int ACCEL, int MODE>
 void launch_closest(const DevScene &s, const MrtRay *rays, uint32_t n, MrtHit *hits, int grid, cudaStream_t q) {
     k_trace_closest<ACCEL, MODE><<<grid, 128, 0, q>>>(s, rays, n, hits);
@@ -150,6 +172,12 @@ int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *
         k_trace_persistent<false><<<persistent_grid(ctx, n), 128, 0, ctx->stream>>>(s->dev, w);
         return cuda_status(ctx, cudaGetLastError(), "k_trace_persistent");
     }
+    if (s->opts.accelerator == MRT_ACCEL_REGULAR_GRID) {
+        cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), ctx->stream);
+        TraceWork<false> w{d_rays, d_hits, nullptr, nullptr, n, ctx->d_counters};
+        k_trace_grid_persistent<<<persistent_grid(ctx, n), 128, 0, ctx->stream>>>(s->dev, w);
+        return cuda_status(ctx, cudaGetLastError(), "k_trace_grid_persistent");
+    }
     MRT_DISPATCH(launch_closest, s->opts.accelerator, s->opts.bvh_mode, s->dev, d_rays, n, d_hits, grid_for(ctx, n), ctx->stream);
     return cuda_status(ctx, cudaGetLastError(), "k_trace_closest");
 }
@@ -168,6 +196,10 @@ int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uin
 
 int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris) {
     MrtContext *ctx = s->ctx;
+    if (s->opts.accelerator == MRT_ACCEL_REGULAR_GRID) {
+        k_trace_counts_grid<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(s->dev, d_rays, n, d_nodes, d_tris);
+        return cuda_status(ctx, cudaGetLastError(), "k_trace_counts_grid");
+    }
     // the same persistent traversal as the render and trace kernels, counting its fetches
     cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), ctx->stream);
     TraceWork<true> w{d_rays, nullptr, d_nodes, d_tris, n, ctx->d_counters};

@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "mrt_gridwalk.cuh"
 #include "mrt_internal.h"
 #include "mrt_paths.cuh"
 
@@ -131,6 +132,15 @@ __global__ void __launch_bounds__(128, 8) k_render_noshadows_fast(DevScene s, Re
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
     persistent_closest<false>(s, w, lane);
+}
+
+// the same work on the RegularGrid: the persistent grid walk (mrt_gridwalk.cuh), one cell per lane
+// and loop iteration
+__global__ void __launch_bounds__(128, 8) k_render_noshadows_grid(DevScene s, RenderParams p, uint32_t first,
+                                                               uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
+    NsWork w{&s, &p, first, count, ctr, tiles_x};
+    NsLane lane;
+    persistent_grid_closest(s, w, lane);
 }
 
 // ============================== wavefront ====================================================
@@ -280,6 +290,14 @@ __global__ void __launch_bounds__(128, 8) k_wave_extend_fast(DevScene s, WaveSta
     ExtendWork work{w, L, ctr};
     WaveLane lane;
     persistent_closest<false>(s, work, lane);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
+}
+
+__global__ void __launch_bounds__(128, 8) k_wave_extend_grid(DevScene s, WaveState w, int level, uint32_t *ctr) {
+    const Level L = clamp_level(w, w.levels[level]);
+    ExtendWork work{w, L, ctr};
+    WaveLane lane;
+    persistent_grid_closest(s, work, lane);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
@@ -476,7 +494,8 @@ void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState
         k_wave_shadow_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level + 1);
         return;
     }
-    k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
+    if (ACCEL == MRT_ACCEL_REGULAR_GRID) k_wave_extend_grid<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
+    else k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
     k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
     k_wave_shadow<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
 }
@@ -593,6 +612,10 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             if (fast) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
+                                                                         plan.round_count[r], ctx->d_counters, tiles_x);
+            } else if (accel == MRT_ACCEL_REGULAR_GRID) {
+                cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
+                k_render_noshadows_grid<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
             } else {
                 MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, plan.round_first[r], plan.round_count[r], grid, q);

@@ -267,8 +267,14 @@ __device__ __forceinline__ bool dda_step(Dda &s) {
     return true;
 }
 
-template <int T>
-__device__ bool grid_trace(const DevScene &s, const Ray &r, float &len, uint32_t &id) {
+// cells visited (start[c], start[c + 1] read) and references tested (refs[k] and the primitive read)
+struct GridCounts {
+    uint32_t cells;
+    uint32_t refs;
+};
+
+template <int T, bool kCount = false>
+__device__ bool grid_trace(const DevScene &s, const Ray &r, float &len, uint32_t &id, GridCounts *cnt = nullptr) {
     const DevGrid &g = s.grid[T];
     if (!g.has) return false;
     Dda st;
@@ -278,8 +284,10 @@ __device__ bool grid_trace(const DevScene &s, const Ray &r, float &len, uint32_t
     for (;;) {
         const uint32_t c = grid_cell(g, st.X, st.Y, st.Z);
         const uint32_t b = g.start[c], e = g.start[c + 1];
+        if (kCount) cnt->cells++;
         bool found = false;
         for (uint32_t k = b; k < e; ++k) {
+            if (kCount) cnt->refs++;
             hit |= prim_hit<T>(s, g.refs[k], r, len, id);
             if (hit) { found = true; break; }
         }
@@ -290,6 +298,7 @@ __device__ bool grid_trace(const DevScene &s, const Ray &r, float &len, uint32_t
     for (;;) {   // testloop, RegularGrid.hpp:282-335
         const uint32_t c = grid_cell(g, st.X, st.Y, st.Z);
         const uint32_t b = g.start[c], e = g.start[c + 1];
+        if (kCount) { cnt->cells++; cnt->refs += e - b; }
         for (uint32_t k = b; k < e; ++k) hit |= prim_hit<T>(s, g.refs[k], r, len, id);
         if (st.tx < st.ty) {
             if (st.tx < st.tz) {

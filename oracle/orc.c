@@ -648,7 +648,8 @@ static int dda_step(Dda *s) {
 }
 
 /* RegularGrid<T>::trace  RegularGrid.hpp:157-337 */
-static int grid_trace(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it) {
+/* counts (optional): cells visited, references tested */
+static int grid_trace_n(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it, uint32_t *cells, uint32_t *refs) {
     if (!g->has) return 0;
     Dda s;
     dda_setup(g, r, &s);
@@ -656,7 +657,9 @@ static int grid_trace(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it)
     for (;;) {
         const uint32_t idx = grid_index(g, s.X, s.Y, s.Z);
         int found = 0;
+        if (cells) ++*cells;
         for (uint32_t k = g->start[idx]; k < g->start[idx + 1]; ++k) {
+            if (refs) ++*refs;
             hit |= ps_hit(ps, g->refs[k], r, it);
             if (hit) { found = 1; break; }
         }
@@ -665,6 +668,8 @@ static int grid_trace(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it)
     }
     for (;;) {   /* testloop  RegularGrid.hpp:282-335 */
         const uint32_t idx = grid_index(g, s.X, s.Y, s.Z);
+        if (cells) ++*cells;
+        if (refs) *refs += g->start[idx + 1] - g->start[idx];
         for (uint32_t k = g->start[idx]; k < g->start[idx + 1]; ++k) hit |= ps_hit(ps, g->refs[k], r, it);
         if (s.tmax[0] < s.tmax[1]) {
             if (s.tmax[0] < s.tmax[2]) {
@@ -685,6 +690,10 @@ static int grid_trace(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it)
         }
     }
     return hit;
+}
+
+static int grid_trace(const Grid *g, const PrimSet *ps, const Ray *r, Isect *it) {
+    return grid_trace_n(g, ps, r, it, NULL, NULL);
 }
 
 /* RegularGrid<T>::shadowTrace  RegularGrid.hpp:340-465 */
@@ -1020,6 +1029,27 @@ void orc_trace_closest(OrcScene *s, const MrtRay *rays, uint32_t n, MrtHit *hits
 void orc_trace_any(OrcScene *s, const MrtRay *rays, const float *dist, uint32_t n, uint8_t *occ, int threads) {
     TraceJob j; j.s = s; j.rays = rays; j.hits = NULL; j.dist = dist; j.occ = occ;
     par_for((long)n, threads, 16, any_body, &j, NULL);
+}
+
+/* the grid walk's work per ray: cells visited and triangle references tested in the triangle grid,
+ * after the plane and sphere grids (the counting replay of the device grid walk) */
+typedef struct { OrcScene *s; const MrtRay *rays; uint32_t *cells, *refs; } CountJob;
+static void count_body(long i, void *vctx, uint64_t *cnt) {
+    CountJob *j = (CountJob *)vctx;
+    const Ray r = ray_from(&j->rays[i]);
+    Isect it;
+    it.length = RAY_LENGTH_MAX; it.id = MRT_HIT_NONE; it.light = -1; it.mat = 0;
+    grid_trace(&j->s->grid[T_PLANE], &j->s->sets[T_PLANE], &r, &it);
+    grid_trace(&j->s->grid[T_SPHERE], &j->s->sets[T_SPHERE], &r, &it);
+    j->cells[i] = 0;
+    j->refs[i] = 0;
+    grid_trace_n(&j->s->grid[T_TRI], &j->s->sets[T_TRI], &r, &it, &j->cells[i], &j->refs[i]);
+}
+int orc_grid_counts(OrcScene *s, const MrtRay *rays, uint32_t n, uint32_t *cells, uint32_t *refs, int threads) {
+    if (s->accel != ORC_ACCEL_GRID) return 1;
+    CountJob j; j.s = s; j.rays = rays; j.cells = cells; j.refs = refs;
+    par_for((long)n, threads, 16, count_body, &j, NULL);
+    return 0;
 }
 
 /* ============================== keyed stream and samplers ===================================== */

@@ -45,6 +45,8 @@ uint64_t orc_scene_bvh_nodes(const OrcScene *s, int type);
 
 void orc_trace_closest(OrcScene *s, const MrtRay *rays, uint32_t n, MrtHit *hits, int threads);
 void orc_trace_any(OrcScene *s, const MrtRay *rays, const float *dist, uint32_t n, uint8_t *occ, int threads);
+/* per ray: cells visited and triangle references tested by the triangle grid (grid scenes only) */
+int orc_grid_counts(OrcScene *s, const MrtRay *rays, uint32_t n, uint32_t *cells, uint32_t *refs, int threads);
 
 /* Whole frame (Renderer::renderFrame restated) with the keyed stream. bitmap: row pitch
  * stride_bytes/4; accum: optional 4 floats per pixel (width*height), summed in sample order. */

@@ -44,6 +44,7 @@ def orc() -> ctypes.CDLL:
             "orc_scene_bvh_nodes": (ctypes.c_uint64, [vp, ip]),
             "orc_trace_closest": (None, [vp, vp, ctypes.c_uint32, vp, ip]),
             "orc_trace_any": (None, [vp, vp, vp, ctypes.c_uint32, vp, ip]),
+            "orc_grid_counts": (ip, [vp, vp, ctypes.c_uint32, vp, vp, ip]),
             "orc_render": (ip, [vp, vp, vp, vp, ctypes.c_uint32, vp, vp, ip]),
             "orc_render_pixels": (ip, [vp, vp, vp, vp, ctypes.c_uint32, vp, ip]),
             "orc_triangle_intersect": (ip, [fp, fp, fp, fp, fp, ctypes.c_float, fp, fp, fp]),
@@ -179,6 +180,15 @@ class OrcScene:
         occ = np.zeros(len(rays), np.uint8)
         self.lib.orc_trace_any(self.h, rays.ctypes.data, dist.ctypes.data, len(rays), occ.ctypes.data, threads)
         return occ
+
+    def grid_counts(self, rays: np.ndarray, threads: int = 8):
+        """(cells visited, triangle references tested) per ray by the triangle grid."""
+        rays = np.ascontiguousarray(rays)
+        cells = np.zeros(len(rays), np.uint32)
+        refs = np.zeros(len(rays), np.uint32)
+        assert self.lib.orc_grid_counts(self.h, rays.ctypes.data, len(rays), cells.ctypes.data, refs.ctypes.data,
+                                        threads) == 0
+        return cells, refs
 
     def render(self, camera, opts, threads: int = 8, bitmap=None, accum=None):
         w, h = opts.width, opts.height

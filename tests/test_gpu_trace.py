@@ -131,3 +131,36 @@ def test_soup_1080p_camera_rays(ctx):
         og = O.OrcScene(sc, 1, grid_size=G, grid_index=index)
         sub = rays[::4]
         assert hits_equal(gg.trace_closest(sub), og.trace_closest(sub)).all(), (G, index)
+
+
+@pytest.mark.parametrize("grid_size,grid_index", [(0, capi.MRT_GRID_INDEX_REFERENCE), (37, capi.MRT_GRID_INDEX_LINEAR)])
+def test_grid_counting_replay_equals_the_oracle_walk(ctx, grid_size, grid_index):
+    """The grid's counting replay (cells visited, triangle references tested: the algorithmic bytes of
+    the grid roofline) equals the oracle's count of the same walk, ray by ray."""
+    sc = scenes.triangle_soup(20000, 3, 320, 240)
+    rays = np.concatenate([random_rays(5000, seed=13), camera_rays(sc.camera, 320, 240, step=7)])
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_REGULAR_GRID, grid_size=grid_size, grid_index=grid_index)
+    cells, refs = g.trace_counts(rays)
+    o = O.OrcScene(sc, 1, grid_size=grid_size, grid_index=grid_index)
+    oc, orf = o.grid_counts(rays)
+    assert np.array_equal(cells, oc) and np.array_equal(refs, orf)
+    assert cells.min() >= 1 and refs.sum() > len(rays)
+
+
+def test_fast_counting_replay_bounds(ctx):
+    """FAST BVH counting replay: a ray that misses the scene's box fetches the root node only; every
+    ray that hits a triangle fetched at least one triangle record."""
+    sc = scenes.triangle_soup(20000, 3, 320, 240)
+    g = Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
+    rays = random_rays(4000, seed=17)
+    miss = np.zeros(2, rays.dtype)
+    miss["origin"] = [[5.0, 5.0, 5.0], [-5.0, 5.0, 5.0]]
+    miss["direction"] = [[0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]
+    miss["depth"] = 1
+    miss["exclude"] = 0xFFFFFFFF
+    rays = np.concatenate([rays, miss])
+    nodes, tris = g.trace_counts(rays)
+    hits = g.trace_closest(rays)
+    assert (tris[-2:] == 0).all() and (nodes[-2:] <= 4).all()
+    hit = (hits["id"] >> 30) == capi.MRT_PRIM_TRIANGLE
+    assert hit.any() and (tris[hit] >= 1).all() and (nodes >= 1).all()
