@@ -27,8 +27,8 @@
  *                         111-139, 338-546) over DrawView's initVerticesArray / initColorsArray /
  *                         initCameraArray (app/System_dependent/Android_JNI/DrawView.cpp:47-210) and
  *                         VertexShaderRaster.glsl / FragmentShaderRaster.glsl
- * mrt_render_noalloc and the mrt_batch_* calls have no counterpart in the reference (the reference
- * renders one frame per Renderer::renderFrame call).
+ * mrt_render_noalloc, the mrt_batch_* and the mrt_serve_* calls have no counterpart in the reference
+ * (the reference renders one frame per Renderer::renderFrame call).
  */
 #ifndef MRT_CUDA_H
 #define MRT_CUDA_H
@@ -399,6 +399,44 @@ int mrt_batch_completed(MrtBatch *batch, uint64_t *ids, uint32_t capacity, uint3
 /* Step until every submitted job is done, then synchronize. */
 int mrt_batch_run(MrtBatch *batch);
 int mrt_batch_stats(const MrtBatch *batch, MrtBatchStats *stats);
+
+/* ---- serving: render requests over time (no counterpart in the reference) -------------------------
+ * Requests arrive while others render; each joins the batched renderer's next waves as soon as its
+ * scene is resident.  Admission by device footprint: a scene is built (on the device, from the host
+ * copy mrt_serve_add_scene made) when its estimated bytes (240 per triangle + 1 MiB, then the exact
+ * size) plus its image fit budget_bytes, after evicting idle resident scenes least recently used
+ * first; otherwise the request waits at the head of the queue.  A scene's image stays resident with
+ * it (and on the host while the scene is evicted): a request with opts->spp_offset > 0 continues the
+ * running mean (a progressive re-render), one with spp_offset 0 starts from a cleared image; requests
+ * of one scene run one at a time in arrival order.  mrt_serve_poll admits, dispatches and launches
+ * waves without waiting for them, and reports finished requests, whose image has been copied to the
+ * host bitmap given at submit (width x height, row pitch 4 * width).  All calls come from one host
+ * thread. */
+typedef struct MrtServe MrtServe;
+typedef struct MrtServeOpts {
+    uint64_t budget_bytes;       /* device bytes for resident scenes and their images */
+    uint64_t build_slack_bytes;  /* further arena bytes for the scratch of the scene being built */
+    MrtBatchOpts batch;          /* the batched renderer behind the requests */
+} MrtServeOpts;
+typedef struct MrtServeStats {
+    uint64_t submitted, completed, builds, evictions;
+    uint64_t resident_bytes, peak_bytes;
+    uint64_t rays_closest, rays_shadow;
+} MrtServeStats;
+int mrt_serve_create(int device, const MrtServeOpts *opts, MrtServe **out);
+void mrt_serve_destroy(MrtServe *serve);
+const char *mrt_serve_error(const MrtServe *serve);
+/* copies the scene's arrays; accel says how its accelerator is built when it becomes resident */
+int mrt_serve_add_scene(MrtServe *serve, const MrtSceneDesc *desc, const MrtAccelOpts *accel, uint64_t *scene_id);
+int mrt_serve_submit(MrtServe *serve, uint64_t scene_id, const MrtCamera *camera, const MrtRenderOpts *opts,
+                     uint32_t *bitmap, uint64_t *request_id);
+/* up to capacity finished request ids in done[], their number in *count */
+int mrt_serve_poll(MrtServe *serve, uint64_t *done, uint32_t capacity, uint32_t *count);
+/* requests submitted and not yet reported by mrt_serve_poll */
+int mrt_serve_pending(const MrtServe *serve, uint64_t *requests);
+/* seconds from mrt_serve_submit to the poll that saw the request finish */
+int mrt_serve_request_latency(const MrtServe *serve, uint64_t request_id, double *seconds);
+int mrt_serve_stats(const MrtServe *serve, MrtServeStats *stats);
 
 #ifdef __cplusplus
 }

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 OUT = os.path.join(OUT_DIR, "libmrt_cuda.so")
 SOURCES = ["mrt_capi.cu", "mrt_bvh.cu", "mrt_grid.cu", "mrt_kernels.cu", "mrt_render.cu", "mrt_batch.cu", "mrt_obj.cu",
-           "mrt_raster.cu"]
+           "mrt_raster.cu", "mrt_serve.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 NVCC_FLAGS = [

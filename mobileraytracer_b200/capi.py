@@ -126,6 +126,16 @@ class MrtBatchStats(ctypes.Structure):
                 ("kernel", ctypes.c_uint32), ("waves_paths", ctypes.c_uint64)]
 
 
+class MrtServeOpts(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("build_slack_bytes", ctypes.c_uint64), ("batch", MrtBatchOpts)]
+
+
+class MrtServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("builds", ctypes.c_uint64),
+                ("evictions", ctypes.c_uint64), ("resident_bytes", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
+                ("rays_closest", ctypes.c_uint64), ("rays_shadow", ctypes.c_uint64)]
+
+
 def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1, pixel_sampler=None,
                 constant_value=0.5, light_sampler=MRT_SAMPLER_RANDOM, rr_sampler=MRT_SAMPLER_RANDOM,
                 depth_min=4, depth_max=8, seed=0, spp_offset=0, depth_point=(1.0, 1.0, 1.0)) -> MrtRenderOpts:
@@ -194,6 +204,16 @@ def load() -> ctypes.CDLL:
         "mrt_render_progress": (ctypes.c_uint32, [vp]),
         "mrt_raster_preview": (ctypes.c_int, [vp, P(MrtCamera), ctypes.c_uint32, ctypes.c_uint32, vp, ctypes.c_uint32,
                                               ctypes.c_uint32, P(MrtRasterStats)]),
+        "mrt_serve_create": (ctypes.c_int, [ctypes.c_int, P(MrtServeOpts), P(vp)]),
+        "mrt_serve_destroy": (None, [vp]),
+        "mrt_serve_error": (ctypes.c_char_p, [vp]),
+        "mrt_serve_add_scene": (ctypes.c_int, [vp, P(MrtSceneDesc), P(MrtAccelOpts), P(ctypes.c_uint64)]),
+        "mrt_serve_submit": (ctypes.c_int, [vp, ctypes.c_uint64, P(MrtCamera), P(MrtRenderOpts), vp,
+                                            P(ctypes.c_uint64)]),
+        "mrt_serve_poll": (ctypes.c_int, [vp, P(ctypes.c_uint64), ctypes.c_uint32, P(ctypes.c_uint32)]),
+        "mrt_serve_pending": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
+        "mrt_serve_request_latency": (ctypes.c_int, [vp, ctypes.c_uint64, P(ctypes.c_double)]),
+        "mrt_serve_stats": (ctypes.c_int, [vp, P(MrtServeStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -210,5 +230,7 @@ EXPORTED_SYMBOLS = [
     "mrt_render_noalloc", "mrt_render_stop", "mrt_render_progress", "mrt_batch_create", "mrt_batch_destroy",
     "mrt_batch_submit", "mrt_batch_step", "mrt_batch_completed", "mrt_batch_run", "mrt_batch_stats",
     "mrt_arena_create", "mrt_arena_destroy", "mrt_arena_stats", "mrt_context_set_arena", "mrt_scene_move",
-    "mrt_obj_load", "mrt_obj_free", "mrt_raster_preview",
+    "mrt_obj_load", "mrt_obj_free", "mrt_raster_preview", "mrt_serve_create", "mrt_serve_destroy", "mrt_serve_error",
+    "mrt_serve_add_scene", "mrt_serve_submit", "mrt_serve_poll", "mrt_serve_pending", "mrt_serve_request_latency",
+    "mrt_serve_stats",
 ]

@@ -32,7 +32,8 @@ def test_library_loads_and_exports_every_declared_symbol():
 
 
 STRUCTS = ["MrtMaterial", "MrtLightDesc", "MrtSceneDesc", "MrtAccelOpts", "MrtRay", "MrtHit", "MrtCamera",
-           "MrtRenderOpts", "MrtRenderStats"]
+           "MrtRenderOpts", "MrtRenderStats", "MrtBatchOpts", "MrtBatchJob", "MrtBatchStats", "MrtServeOpts",
+           "MrtServeStats"]
 
 
 def test_struct_layouts_match_the_header(tmp_path):
