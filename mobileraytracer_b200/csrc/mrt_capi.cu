@@ -333,6 +333,10 @@ int mrt_scene_create(MrtContext *ctx, const MrtSceneDesc *d, MrtScene **out) {
     s->n_pln = d->n_planes;
     s->n_light = d->n_lights;
     s->n_mat = d->n_materials;
+    for (uint32_t k = 0; k < d->n_materials; ++k) {
+        const MrtMaterial &m = d->materials[k];
+        if (m.ks[0] > 0 || m.ks[1] > 0 || m.ks[2] > 0 || m.kt[0] > 0 || m.kt[1] > 0 || m.kt[2] > 0) s->mixed_materials = true;
+    }
     const uint32_t nt = s->n_tri;
     int st = MRT_OK;
     auto alloc = [&](DevBuf &b, size_t bytes) { if (st == MRT_OK) st = dev_alloc(ctx, b, bytes); };

@@ -64,6 +64,7 @@ struct MrtScene {
     // geometry
     uint32_t n_tri = 0, n_sph = 0, n_pln = 0, n_light = 0, n_mat = 0;
     DevBuf tri_a, tri_ab, tri_ac, tri_n, tri_c, tri_mat, sph, sph_mat, pln_n, pln_p, pln_mat, lights, mats;
+    bool mixed_materials = false;       // some material reflects or transmits (per-material shade queues)
     // accelerators
     bool built = false;
     MrtAccelOpts opts{};

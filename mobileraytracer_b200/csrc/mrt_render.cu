@@ -60,6 +60,12 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
     }
 }
 
+// per-material shade queues in the wavefront of scenes that mix materials (0 builds without them)
+#ifndef MRT_SHADE_QUEUES
+#define MRT_SHADE_QUEUES 1
+#endif
+constexpr bool kShadeQueues = MRT_SHADE_QUEUES != 0;
+
 // persistent FAST-BVH NoShadows: work item = pixel task; the lane traces the pixel's samples in
 // order.  Only the task number and the sample count stay in registers while a ray is traced: the
 // pixel's running mean and fp32 sums are read and written back at the end of each sample (a few
@@ -183,16 +189,52 @@ __global__ void __launch_bounds__(128) k_wave_extend(DevScene s, WaveState w, in
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
+// the level's rays sorted into the per-material shade queues: one atomic per warp and class
+// (warp ballot over the class, popc for the lane's rank)
+__global__ void __launch_bounds__(128) k_wave_classify(DevScene s, RenderParams p, WaveState w, int level) {
+    const Level L = clamp_level(w, w.levels[level]);
+    const uint32_t n_iter = (L.count + blockDim.x - 1) / blockDim.x;
+    const int lane = threadIdx.x & 31;
+    uint32_t *count = w.class_count + kShadeClasses * level;
+    for (uint32_t it_ = blockIdx.x; it_ < n_iter; it_ += gridDim.x) {
+        const uint32_t i = it_ * blockDim.x + threadIdx.x;
+        const bool active = i < L.count;
+        const uint32_t idx = L.start + (active ? i : 0u);
+        const uint32_t c = active ? shade_class(s, p, w.rays[idx], w.nodes[idx].hit_id) : 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < (uint32_t)kShadeClasses; ++k) {
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, active && c == k);
+            if (!mask) continue;
+            const int leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&count[k], (uint32_t)__popc(mask));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (active && c == k) {
+                const uint32_t pos = base + __popc(mask & ((1u << lane) - 1u));
+                if (pos < w.order_cap) w.order[(size_t)k * w.order_cap + pos] = idx;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_wave_shade(DevScene s, RenderParams p, WaveState w, int level) {
     const Level L = clamp_level(w, w.levels[level]);
     Level *next = &w.levels[level + 1];
     if (blockIdx.x == 0 && threadIdx.x == 0) next->start = L.start + L.count;
     const uint32_t next_start = L.start + L.count;
     const uint32_t n_iter = (L.count + blockDim.x - 1) / blockDim.x;   // whole warps iterate together
+    uint32_t qn[kShadeClasses] = {0, 0, 0};
+    if (w.order)
+        for (int k = 0; k < kShadeClasses; ++k) qn[k] = min(w.class_count[kShadeClasses * level + k], w.order_cap);
     for (uint32_t it_ = blockIdx.x; it_ < n_iter; it_ += gridDim.x) {
         const uint32_t i = it_ * blockDim.x + threadIdx.x;
         const bool active = i < L.count;
-        const uint32_t idx = L.start + (active ? i : 0);
+        uint32_t idx = L.start + (active ? i : 0);
+        if (w.order && active) {   // the i-th ray of the queues in class order
+            if (i < qn[0]) idx = w.order[i];
+            else if (i < qn[0] + qn[1]) idx = w.order[(size_t)w.order_cap + (i - qn[0])];
+            else if (i < qn[0] + qn[1] + qn[2]) idx = w.order[2 * (size_t)w.order_cap + (i - qn[0] - qn[1])];
+        }
         ShadeLane o;
         o.n_child = 0;
         o.n_shadow = 0;
@@ -490,12 +532,14 @@ void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState
     if (ACCEL == MRT_ACCEL_BVH && MODE == MRT_BVH_FAST) {
         // counters [2 * level] and [2 * level + 1] were zeroed for this wave
         k_wave_extend_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
+        if (w.order) k_wave_classify<<<grid, 128, 0, q>>>(s, p, w, level);
         k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
         k_wave_shadow_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level + 1);
         return;
     }
     if (ACCEL == MRT_ACCEL_REGULAR_GRID) k_wave_extend_grid<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
     else k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
+    if (w.order) k_wave_classify<<<grid, 128, 0, q>>>(s, p, w, level);
     k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
     k_wave_shadow<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
 }
@@ -646,6 +690,10 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[4], sizeof(Level) * (levels + 2));
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[5], sizeof(float4) * wave);
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[6], 16);
+        // per-material shade queues where the scene mixes diffuse with mirror / glass materials
+        const bool queues = kShadeQueues && !paths && s->mixed_materials;
+        if (queues && st == MRT_OK)
+            st = ensure(ctx, ctx->wave[0], 4ull * kShadeClasses * (ray_cap + (uint64_t)levels + 1));
         if (st != MRT_OK) return st;
         WaveState w{};
         w.rays = (RayRec *)ctx->wave[1].ptr;
@@ -656,6 +704,11 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         w.counters = (unsigned long long *)ctx->wave[6].ptr;
         w.ray_cap = (uint32_t)ray_cap;
         w.shadow_cap = (uint32_t)shadow_cap;
+        if (queues) {
+            w.order = (uint32_t *)ctx->wave[0].ptr;
+            w.order_cap = (uint32_t)ray_cap;
+            w.class_count = w.order + (size_t)kShadeClasses * ray_cap;
+        }
         cudaMemsetAsync(w.counters, 0, 16, q);
         // at most one wave queued ahead of the one running: a stop request ends the render within two
         // waves, and progress counts finished waves
@@ -680,6 +733,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 } else {
                     cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
                     cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
+                    if (w.class_count) cudaMemsetAsync(w.class_count, 0, 4ull * kShadeClasses * (levels + 1), q);
                     k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
                     for (int b = 0; b < levels; ++b)
                         MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);

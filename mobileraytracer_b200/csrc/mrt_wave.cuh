@@ -185,7 +185,32 @@ struct WaveState {
     uint32_t root_first;     // global index of the wave's first root
     uint32_t n_roots;
     unsigned long long *counters;   // [0] closest rays, [1] shadow rays
+    // per-material shade queues (nullptr: the shade kernel takes the level's rays in order): after
+    // the closest hits of a level, its rays are sorted by shading class (kShadeClasses queues of
+    // order_cap entries, their lengths in class_count[kShadeClasses * level + c]) so that the warps
+    // of the shade kernel run one material branch each
+    uint32_t *order;
+    uint32_t *class_count;
+    uint32_t order_cap;
 };
+
+// shading class of a ray after its closest hit: 0 nothing to shade here (a miss, a ray beyond the
+// depth limit, an emitter), 1 diffuse only (light samples and the hemisphere ray), 2 a specular
+// or transmitting material (mirror / refraction rays, Whitted.cpp:85-104, PathTracer.cpp:136-157)
+constexpr int kShadeClasses = 3;
+__device__ __forceinline__ uint32_t shade_class(const DevScene &s, const RenderParams &p, const RayRec &rr, uint32_t hit_id) {
+    if (hit_id == MRT_HIT_NONE || rr.depth > p.depth_max) return 0u;
+    const uint32_t type = MRT_HIT_TYPE(hit_id), i = MRT_HIT_INDEX(hit_id);
+    int32_t m = -1;
+    if (type == MRT_PRIM_TRIANGLE) m = s.tri_mat[i];
+    else if (type == MRT_PRIM_SPHERE) m = s.sph_mat[i];
+    else if (type == MRT_PRIM_PLANE) m = s.pln_mat[i];
+    else return 0u;   // an area light: an emitter
+    if (m < 0 || (uint32_t)m >= s.n_mat) return 1u;   // the primitive's colour: diffuse
+    const DevMaterial &mt = s.mats[m];
+    if (any_pos(mt.le)) return 0u;
+    return (any_pos(mt.ks) || any_pos(mt.kt)) ? 2u : 1u;
+}
 
 __device__ __forceinline__ uint32_t warp_alloc(uint32_t want, uint32_t *counter) {
     // warp-aggregated allocation: inclusive scan of `want` across the warp, one atomic per warp.

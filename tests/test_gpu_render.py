@@ -261,3 +261,16 @@ def test_whole_paths_equal_wavefront(ctx, tmp_path):
         assert np.array_equal(bm, wf[f"arr_{3 * k}"])
         assert np.array_equal(acc.view(np.uint32), wf[f"arr_{3 * k + 1}"].view(np.uint32))
         assert [st.rays_closest, st.rays_shadow] == list(wf[f"arr_{3 * k + 2}"])
+
+
+@pytest.mark.parametrize("shader", [WH, PT])
+def test_glass_room_wavefront_with_material_queues(ctx, shader):
+    """A frame above the whole-path limit (768x768 = 589,824 camera paths) of a scene that mixes
+    diffuse walls with mirror and glass spheres: the FAST-BVH wavefront sorts every level's rays into
+    per-material shade queues.  The result equals the oracle bit for bit."""
+    sc = scenes.glass_room()
+    opts = capi.render_opts(shader=shader, width=768, height=768, spp=1, spl=1, seed=4)
+    bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, capi.MRT_ACCEL_BVH,
+                                                          capi.MRT_BVH_FAST, 3)
+    assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3 if shader == PT else 1e-4)
+    assert stats.rays_closest == counts[0] and stats.rays_shadow == counts[1]
