@@ -42,7 +42,7 @@ FRAME = "NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point ligh
 WORKLOAD = FRAME + ", FAST BVH built on the device"
 REF_WORKLOAD = FRAME + ", the reference's BVH (BVH<Triangle>, top-down SAH) built on the host"
 PROFILE = os.path.join(ROOT, "profiles", "render_noshadows_soup_1080p.md")
-FAST_NODE_BYTES = 32   # bytes per node record the FAST tree's counting replay counts
+FAST_NODE_BYTES = 128  # bytes of one 8-wide node, the unit of the FAST tree's counting replay
 
 
 def log(*a):

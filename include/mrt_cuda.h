@@ -58,8 +58,9 @@ extern "C" {
 /* BVH flavour.  REFERENCE rebuilds the reference tree (unsorted top-down SAH, leaf <= 2,
  * BVH.hpp:87-155,273-311) and walks it with the reference slab test in the reference order, so its
  * results equal BVH<T>::trace bit for bit, including the slab test's rejections.  FAST builds a
- * Morton-ordered tree on the device and walks it front to back with a conservative slab test; its
- * closest hit is the exact closest hit (= Naive<T>), ties resolved to the lowest primitive index. */
+ * Morton-ordered tree on the device, compressed into 8-wide nodes with quantised boxes, and walks it
+ * nearest child first with a conservative box test; its closest hit is the exact closest hit
+ * (= Naive<T>), ties resolved to the lowest primitive index. */
 #define MRT_BVH_FAST 0
 #define MRT_BVH_REFERENCE 1
 
@@ -251,7 +252,8 @@ int mrt_scene_build(MrtScene *scene, const MrtAccelOpts *opts);
 int mrt_scene_move(MrtScene *scene, MrtContext *ctx);
 /* Device bytes held by the scene (geometry + accelerator), for footprint admission. */
 uint64_t mrt_scene_device_bytes(const MrtScene *scene);
-/* Accelerator statistics: nodes (BVH records) or cells (grid), references, grid size. */
+/* Accelerator statistics: nodes (reference BVH nodes, or 8-wide FAST nodes) or cells (grid),
+ * references, grid size. */
 int mrt_scene_accel_info(const MrtScene *scene, uint64_t *nodes, uint64_t *refs, int32_t *grid_size);
 
 /* ---- scene files ---------------------------------------------------------------------------- */
@@ -272,7 +274,7 @@ int mrt_trace_closest(MrtScene *scene, const MrtRay *rays, uint32_t n, MrtHit *h
 /* occluded[i] = 1 if any plane/sphere/triangle blocks rays[i] within (Epsilon, dist[i]) */
 int mrt_trace_any(MrtScene *scene, const MrtRay *rays, const float *dist, uint32_t n,
                   uint8_t *occluded, uint32_t mem);
-/* Counting replay of mrt_trace_closest: per ray, on the FAST BVH the 32-byte child records and the
+/* Counting replay of mrt_trace_closest: per ray, on the FAST BVH the 128-byte nodes and the
  * 48-byte triangle records fetched; on the regular grid the cells visited (node_fetch) and the
  * triangle references tested (tri_fetch).  Other accelerators return MRT_ERR_STATE. */
 int mrt_trace_closest_counts(MrtScene *scene, const MrtRay *rays, uint32_t n, uint32_t *node_fetch,

@@ -7,12 +7,13 @@
 // FAST tree: built on the device.  Triangle boxes padded outward -> 30-bit Morton codes of the
 // centroids -> stable LSD radix sort (own kernels) -> Karras' parallel hierarchy ("Maximizing
 // parallelism in the construction of BVHs, octrees and k-d trees", HPG 2012) -> bottom-up box fit
-// -> records in child-pair layout (32 bytes per record), subtrees of <= leaf_max_setting()
+// -> records in child-pair layout (32 bytes per record), subtrees of <= leaf_max_setting() (at most 3)
 // triangles collapsed into leaves where the surface-area cost says so -> the binary tree collapsed
-// into kWide-wide nodes (one 128-byte node = the kWide child records a traversal step tests; each
-// wide node opens the largest internal children of a binary node until it is full), wide nodes
-// numbered level by level -> triangles copied in leaf order as 48-byte records.  A traversal step of the wide tree replaces about two of the binary
-// tree's, halving the chain of dependent node fetches per ray.
+// into 8-wide nodes with 16-bit quantised child boxes (128 bytes: one cache line per traversal step;
+// each wide node opens the largest internal children of a binary node until it holds 8), children
+// placed in slots by octant, internal children numbered consecutively, the leaf children's triangles
+// copied to consecutive 48-byte records.  A traversal step of the 8-wide tree replaces about three of
+// the binary tree's, shortening the chain of dependent node fetches per ray.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -434,73 +435,151 @@ __global__ void k_single_leaf(const float4 *bmin, const float4 *bmax, float4 *re
     write_record(records, bmin[0], bmax[0], 0u, 1u);
 }
 
-// ------------------------------ binary -> wide collapse ---------------------------------------
+// ------------------------------ binary -> 8-wide compressed nodes ------------------------------
+// Each wide node starts from the children of one binary internal node (or from the root record) and
+// opens its largest-area internal child until it holds kWide children.  Its box is the union of the
+// children's boxes; per axis the children's planes are quantised on a grid p + 2^E q (16-bit q,
+// lo rounded down and hi up, so every quantised box contains the exact one), the children are
+// placed in slots by the octant of their centre within the node, internal children get consecutive
+// node indices (one allocation per node), and the triangles of the leaf children are copied to
+// consecutive records (one allocation per node).  One launch per level of the wide tree.
 struct CollapseItem {
-    uint32_t bin;    // binary internal node (children at records 2 + 2 bin, 3 + 2 bin)
-    uint32_t wide;   // wide node it becomes
+    uint32_t rec;     // first seed record: the root record 0 (one seed) or a child pair 2 + 2k (two seeds)
+    uint32_t seeds;   // 1 or 2
+    uint32_t node;    // the wide node it becomes
 };
 
-__device__ __forceinline__ void write_empty_slot(float4 *rec) {
-    rec[0] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
-    rec[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+__device__ __forceinline__ bool rec_internal(const float4 *bin, uint32_t r) { return __float_as_int(bin[2 * (size_t)r + 1].w) == 0; }
+
+// grid step exponent E of one axis (2^E >= extent / 65534)
+__device__ __forceinline__ int grid_exponent(float lo, float hi) {
+    const double want = ((double)hi - (double)lo) / 65534.0;
+    if (!(want > 0x1p-126)) return -126;
+    int ex = 0;
+    const double m = frexp(want, &ex);   // want = m 2^ex, m in [0.5, 1)
+    return m == 0.5 ? ex - 1 : ex;
+}
+// a child's planes on the grid, lo rounded down and hi up (with a 2^-20 step guard against the
+// rounding of the double-precision subtraction), as lo | hi << 16
+__device__ __forceinline__ uint32_t quantise(float p, double step, float lo, float hi) {
+    double ql = floor(((double)lo - (double)p) / step - 0x1p-20);
+    double qh = ceil(((double)hi - (double)p) / step + 0x1p-20);
+    ql = fmin(fmax(ql, 0.0), 65535.0);
+    qh = fmin(fmax(qh, 0.0), 65535.0);
+    return (uint32_t)ql | ((uint32_t)qh << 16);
 }
 
-// the root: a leaf root becomes slot 0 of wide node 0; an internal root is the first item
-__global__ void k_collapse_root(const float4 *bin, float4 *wide, CollapseItem *queue, uint32_t *ctrs) {
-    const float4 lo = bin[0], hi = bin[1];
-    if (__float_as_int(hi.w) > 0) {
-        write_record(wide, lo, hi, leaf_code(__float_as_uint(lo.w), (uint32_t)__float_as_int(hi.w)),
-                     (uint32_t)__float_as_int(hi.w));
-        for (int k = 1; k < kWide; ++k) write_empty_slot(wide + 2 * k);
-        ctrs[0] = 0;   // next level: empty
-    } else {
-        queue[0] = CollapseItem{0u, 0u};
-        ctrs[0] = 1;
-    }
-    ctrs[1] = 1;       // wide nodes allocated
-}
-
-// one level: every item's binary node becomes a wide node; its internal slots get wide nodes of
-// the next level.  ctrs[0]: items of the next level, ctrs[1]: wide nodes, ctrs[2]: error
+// ctrs[0]: items of the next level, [1]: nodes allocated, [2]: error, [3]: triangles placed
 __global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, const CollapseItem *__restrict__ in,
-                           uint32_t n_in, CollapseItem *out, uint32_t cap, float4 *wide, uint32_t *ctrs) {
+                           uint32_t n_in, CollapseItem *out, uint32_t cap, uint4 *nodes, const float4 *__restrict__ mtris,
+                           float4 *tris, uint32_t n_tri, uint32_t *ctrs) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_in) return;
     const CollapseItem it = in[i];
     uint32_t rec[kWide];
-    int m = 2;
-    rec[0] = 2u + 2u * it.bin;
-    rec[1] = rec[0] + 1u;
-    if ((uint64_t)rec[1] >= n_records) { atomicMax(&ctrs[2], 1u); return; }
-    for (;;) {   // open the internal slot with the largest box while there is room
+    int m = (int)it.seeds;
+    rec[0] = it.rec;
+    rec[1] = it.rec + 1u;
+    if ((uint64_t)it.rec + (uint64_t)it.seeds > n_records || it.node >= cap) { atomicMax(&ctrs[2], 1u); return; }
+    for (;;) {   // open the internal child with the largest box while there is room
         if (m >= kWide) break;
         int best = -1;
         float best_area = -1.0f;
         for (int k = 0; k < m; ++k) {
-            const float4 lo = bin[2 * (size_t)rec[k]], hi = bin[2 * (size_t)rec[k] + 1];
-            if (__float_as_int(hi.w) != 0) continue;
-            const float a = half_area(lo, hi);
+            if (!rec_internal(bin, rec[k])) continue;
+            const float a = half_area(bin[2 * (size_t)rec[k]], bin[2 * (size_t)rec[k] + 1]);
             if (a > best_area) { best_area = a; best = k; }
         }
         if (best < 0) break;
         const uint32_t a = __float_as_uint(bin[2 * (size_t)rec[best]].w);
-        if ((uint64_t)a + 1u >= n_records) { atomicMax(&ctrs[2], 1u); return; }
+        if (a < 2u || (uint64_t)a + 1u >= n_records) { atomicMax(&ctrs[2], 1u); return; }
         rec[best] = a;
         rec[m++] = a + 1u;
     }
-    float4 *node = wide + (size_t)it.wide * (2 * kWide);
-    for (int k = 0; k < kWide; ++k) {
-        if (k >= m) { write_empty_slot(node + 2 * k); continue; }
-        const float4 lo = bin[2 * (size_t)rec[k]], hi = bin[2 * (size_t)rec[k] + 1];
-        const int b = __float_as_int(hi.w);
-        if (b > 0) { write_record(node + 2 * k, lo, hi, leaf_code(__float_as_uint(lo.w), (uint32_t)b), (uint32_t)b); continue; }
-        const uint32_t a = __float_as_uint(lo.w);
-        const uint32_t j = atomicAdd(&ctrs[1], 1u);
-        const uint32_t q = atomicAdd(&ctrs[0], 1u);
-        if (j >= cap || q >= cap || a < 2u) { atomicMax(&ctrs[2], 1u); write_empty_slot(node + 2 * k); continue; }
-        out[q] = CollapseItem{(a - 2u) / 2u, j};
-        write_record(node + 2 * k, lo, hi, j, 0u);
+    float4 lo[kWide], hi[kWide];
+    float4 nlo = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.0f), nhi = make_float4(-3.0e38f, -3.0e38f, -3.0e38f, 0.0f);
+    for (int k = 0; k < m; ++k) {
+        lo[k] = bin[2 * (size_t)rec[k]];
+        hi[k] = bin[2 * (size_t)rec[k] + 1];
+        nlo = make_float4(fminf(nlo.x, lo[k].x), fminf(nlo.y, lo[k].y), fminf(nlo.z, lo[k].z), 0.0f);
+        nhi = make_float4(fmaxf(nhi.x, hi[k].x), fmaxf(nhi.y, hi[k].y), fmaxf(nhi.z, hi[k].z), 0.0f);
     }
+    // slots by octant: the child whose centre lies on the high side of axis a prefers slots with bit a set
+    const float cx = 0.5f * (nlo.x + nhi.x), cy = 0.5f * (nlo.y + nhi.y), cz = 0.5f * (nlo.z + nhi.z);
+    int slot_of[kWide];
+    uint32_t used = 0, placed = 0;
+    for (int k = 0; k < m; ++k) slot_of[k] = -1;
+    for (int round = 0; round < m; ++round) {
+        float best = 3.0e38f;
+        int bk = -1, bs = -1;
+        for (int k = 0; k < m; ++k) {
+            if ((placed >> k) & 1u) continue;
+            const float dx = 0.5f * (lo[k].x + hi[k].x) - cx, dy = 0.5f * (lo[k].y + hi[k].y) - cy,
+                        dz = 0.5f * (lo[k].z + hi[k].z) - cz;
+            for (int sl = 0; sl < kWide; ++sl) {
+                if ((used >> sl) & 1u) continue;
+                const float c = ((sl & 1) ? -dx : dx) + ((sl & 2) ? -dy : dy) + ((sl & 4) ? -dz : dz);
+                if (c < best) { best = c; bk = k; bs = sl; }
+            }
+        }
+        if (bk < 0) {   // non-finite centres: the first free slot
+            bk = __ffs(~placed & ((1u << m) - 1u)) - 1;
+            bs = __ffs(~used & 0xFFu) - 1;
+        }
+        slot_of[bk] = bs;
+        placed |= 1u << bk;
+        used |= 1u << bs;
+    }
+    int child_at[kWide];
+    for (int sl = 0; sl < kWide; ++sl) child_at[sl] = -1;
+    uint32_t imask = 0, n_int = 0, n_lt = 0;
+    for (int k = 0; k < m; ++k) {
+        child_at[slot_of[k]] = k;
+        if (rec_internal(bin, rec[k])) { imask |= 1u << slot_of[k]; ++n_int; }
+        else n_lt += (uint32_t)__float_as_int(hi[k].w);
+    }
+    const uint32_t child_base = n_int ? atomicAdd(&ctrs[1], n_int) : 0u;
+    const uint32_t qpos = n_int ? atomicAdd(&ctrs[0], n_int) : 0u;
+    const uint32_t tri_base = n_lt ? atomicAdd(&ctrs[3], n_lt) : 0u;
+    if ((uint64_t)child_base + n_int > cap || (uint64_t)qpos + n_int > cap || (uint64_t)tri_base + n_lt > n_tri) {
+        atomicMax(&ctrs[2], 1u);
+        return;
+    }
+    const int ex = grid_exponent(nlo.x, nhi.x), ey = grid_exponent(nlo.y, nhi.y), ez = grid_exponent(nlo.z, nhi.z);
+    if (ex > 127 || ey > 127 || ez > 127) { atomicMax(&ctrs[2], 2u); return; }
+    const double sx = ldexp(1.0, ex), sy = ldexp(1.0, ey), sz = ldexp(1.0, ez);
+    uint32_t w[kNodeWords];
+    w[0] = __float_as_uint(nlo.x);
+    w[1] = __float_as_uint(nlo.y);
+    w[2] = __float_as_uint(nlo.z);
+    w[3] = (uint32_t)(ex + 127) | ((uint32_t)(ey + 127) << 8) | ((uint32_t)(ez + 127) << 16) | (imask << 24);
+    w[4] = child_base;
+    w[5] = tri_base;
+    w[6] = w[7] = 0;
+    uint32_t offset = 0, rank = 0;
+    for (int sl = 0; sl < kWide; ++sl) {
+        const int k = child_at[sl];
+        if (k < 0) {   // empty slot: an inverted box, no meta
+            w[8 + sl] = w[16 + sl] = w[24 + sl] = 0xFFFFu;
+            continue;
+        }
+        w[8 + sl] = quantise(nlo.x, sx, lo[k].x, hi[k].x);
+        w[16 + sl] = quantise(nlo.y, sy, lo[k].y, hi[k].y);
+        w[24 + sl] = quantise(nlo.z, sz, lo[k].z, hi[k].z);
+        if ((imask >> sl) & 1u) {
+            out[qpos + rank] = CollapseItem{__float_as_uint(lo[k].w), 2u, child_base + rank};
+            ++rank;
+        } else {
+            const uint32_t first = __float_as_uint(lo[k].w), count = (uint32_t)__float_as_int(hi[k].w);
+            if (count == 0 || count > kMaxLeafTris || (uint64_t)first + count > n_tri) { atomicMax(&ctrs[2], 1u); return; }
+            w[6 + (sl >> 2)] |= ((((1u << count) - 1u) << 5) | offset) << (8 * (sl & 3));
+            for (uint32_t j = 0; j < count; ++j)
+                for (int c = 0; c < 3; ++c) tris[3 * (size_t)(tri_base + offset + j) + c] = mtris[3 * (size_t)(first + j) + c];
+            offset += count;
+        }
+    }
+    uint4 *dst = nodes + (size_t)it.node * (kNodeWords / 4);
+    for (int q = 0; q < kNodeWords / 4; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
 }
 
 }  // namespace
@@ -510,8 +589,8 @@ namespace mrt_host {
 int leaf_max_setting() {
     static int v = [] {
         const char *e = getenv("MRT_BVH_LEAF_MAX");
-        const int x = e ? atoi(e) : 4;   // the largest subtree the surface-area leaf choice may keep as one leaf
-        return x < 1 ? 1 : (x > 16 ? 16 : x);
+        const int x = e ? atoi(e) : (int)kMaxLeafTris;   // the largest subtree the surface-area leaf choice may keep as one leaf
+        return x < 1 ? 1 : (x > (int)kMaxLeafTris ? (int)kMaxLeafTris : x);
     }();
     return v;
 }
@@ -528,8 +607,8 @@ int build_fast_bvh(MrtScene *s) {
         s->dev.ftris = nullptr;
         return MRT_OK;
     }
-    if (n >= kMaxLeafFirst) {
-        set_error(ctx, "fast bvh: at most %u triangles", kMaxLeafFirst - 1u);
+    if (n >= kMaxFastTris) {
+        set_error(ctx, "fast bvh: at most %u triangles", kMaxFastTris - 1u);
         return MRT_ERR_ARG;
     }
     int st = MRT_OK;
@@ -537,7 +616,7 @@ int build_fast_bvh(MrtScene *s) {
     st = dev_alloc(ctx, s->fnodes, 32ull * n_records);
     if (st == MRT_OK) st = dev_alloc(ctx, s->ftris, 48ull * n);
     if (st != MRT_OK) return st;
-    DevBuf bmin, bmax, cb, keys[2], vals[2], hist, lft, rgt, fst, lst, pint, pleaf, ctr, imin, imax;
+    DevBuf bmin, bmax, cb, keys[2], vals[2], hist, lft, rgt, fst, lst, pint, pleaf, ctr, imin, imax, mtris;
     const uint32_t nblocks = (n + kSortTile - 1) / kSortTile;
     auto A = [&](DevBuf &b, size_t bytes) { if (st == MRT_OK) st = dev_alloc(ctx, b, bytes); };
     A(bmin, 16ull * n); A(bmax, 16ull * n); A(cb, 64);
@@ -545,6 +624,7 @@ int build_fast_bvh(MrtScene *s) {
     A(hist, 4ull * 256 * nblocks);
     A(lft, 4ull * n); A(rgt, 4ull * n); A(fst, 4ull * n); A(lst, 4ull * n);
     A(pint, 4ull * n); A(pleaf, 4ull * n); A(ctr, 4ull * n); A(imin, 16ull * n); A(imax, 16ull * n);
+    A(mtris, 48ull * n);
     if (st == MRT_OK) {
         const uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
         st = cuda_status(ctx, cudaMemcpyAsync(cb.ptr, init, sizeof(init), cudaMemcpyHostToDevice, q), "bvh init");
@@ -584,28 +664,26 @@ int build_fast_bvh(MrtScene *s) {
                                                        (const float4 *)imax.ptr, (float4 *)s->fnodes.ptr);
         }
         k_leaf_tris<<<(n + 255) / 256, 256, 0, q>>>(n, svals, s->dev.tri_a, s->dev.tri_ab, s->dev.tri_ac,
-                                                    (float4 *)s->ftris.ptr);
+                                                    (float4 *)mtris.ptr);
         st = cuda_status(ctx, cudaGetLastError(), "fast bvh kernels");
         if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "fast bvh build");
     }
     DevBuf *tmp[] = {&bmin, &bmax, &cb, &keys[0], &keys[1], &vals[0], &vals[1], &hist, &lft, &rgt, &fst, &lst,
                      &pint, &pleaf, &ctr, &imin, &imax};
     for (DevBuf *b : tmp) dev_free(*b);
-    if (st != MRT_OK) return st;
-    // collapse into wide nodes, level by level
+    if (st != MRT_OK) { dev_free(mtris); return st; }
+    // collapse into 8-wide compressed nodes, level by level, from the root record
     DevBuf wide, queue[2], wctr;
     const uint32_t cap = n;   // wide nodes <= binary internal nodes + 1
-    A(wide, 32ull * kWide * cap);
+    A(wide, 4ull * kNodeWords * cap);
     A(queue[0], sizeof(CollapseItem) * cap);
     A(queue[1], sizeof(CollapseItem) * cap);
     A(wctr, 16);
-    uint32_t h[3] = {0, 0, 0};
+    uint32_t h[4] = {1, 1, 0, 0};   // the root item, the root node
     if (st == MRT_OK) {
-        cudaMemsetAsync(wctr.ptr, 0, 16, q);
-        k_collapse_root<<<1, 1, 0, q>>>((const float4 *)s->fnodes.ptr, (float4 *)wide.ptr, (CollapseItem *)queue[0].ptr,
-                                        (uint32_t *)wctr.ptr);
-        st = cuda_status(ctx, cudaMemcpyAsync(h, wctr.ptr, 12, cudaMemcpyDeviceToHost, q), "collapse");
-        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse");
+        const CollapseItem root{0u, 1u, 0u};
+        st = cuda_status(ctx, cudaMemcpyAsync(queue[0].ptr, &root, sizeof(root), cudaMemcpyHostToDevice, q), "collapse");
+        if (st == MRT_OK) st = cuda_status(ctx, cudaMemcpyAsync(wctr.ptr, h, 16, cudaMemcpyHostToDevice, q), "collapse");
     }
     int cur_q = 0;
     for (int level = 0; st == MRT_OK && h[0] > 0 && h[2] == 0; ++level) {
@@ -614,30 +692,32 @@ int build_fast_bvh(MrtScene *s) {
         cudaMemsetAsync(wctr.ptr, 0, 4, q);
         k_collapse<<<(n_in + 127) / 128, 128, 0, q>>>((const float4 *)s->fnodes.ptr, (uint32_t)n_records,
                                                        (const CollapseItem *)queue[cur_q].ptr, n_in,
-                                                       (CollapseItem *)queue[1 - cur_q].ptr, cap, (float4 *)wide.ptr,
+                                                       (CollapseItem *)queue[1 - cur_q].ptr, cap, (uint4 *)wide.ptr,
+                                                       (const float4 *)mtris.ptr, (float4 *)s->ftris.ptr, n,
                                                        (uint32_t *)wctr.ptr);
         cur_q = 1 - cur_q;
-        st = cuda_status(ctx, cudaMemcpyAsync(h, wctr.ptr, 12, cudaMemcpyDeviceToHost, q), "collapse");
+        st = cuda_status(ctx, cudaMemcpyAsync(h, wctr.ptr, 16, cudaMemcpyDeviceToHost, q), "collapse");
         if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse");
     }
-    if (st == MRT_OK && h[2] != 0) {
-        set_error(ctx, "fast bvh: inconsistent binary tree while collapsing");
+    if (st == MRT_OK && (h[2] != 0 || h[3] != n)) {
+        set_error(ctx, h[2] == 2 ? "fast bvh: scene extent beyond the 2^127 grid step"
+                                 : "fast bvh: inconsistent binary tree while collapsing");
         st = MRT_ERR_LIMIT;
     }
     const uint64_t n_wide = h[1];
     if (st == MRT_OK) {   // exact-size copy; the binary records and the scratch go
         dev_free(s->fnodes);
-        st = dev_alloc(ctx, s->fnodes, 32ull * kWide * n_wide);
+        st = dev_alloc(ctx, s->fnodes, 4ull * kNodeWords * n_wide);
         if (st == MRT_OK)
-            st = cuda_status(ctx, cudaMemcpyAsync(s->fnodes.ptr, wide.ptr, 32ull * kWide * n_wide,
+            st = cuda_status(ctx, cudaMemcpyAsync(s->fnodes.ptr, wide.ptr, 4ull * kNodeWords * n_wide,
                                                   cudaMemcpyDeviceToDevice, q), "collapse copy");
         if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(q), "collapse copy");
     }
-    DevBuf *tmp2[] = {&wide, &queue[0], &queue[1], &wctr};
+    DevBuf *tmp2[] = {&wide, &queue[0], &queue[1], &wctr, &mtris};
     for (DevBuf *b : tmp2) dev_free(*b);
     if (st != MRT_OK) return st;
-    s->fnode_count = n_wide * kWide;
-    s->dev.n_fnodes = (uint32_t)(n_wide * kWide);
+    s->fnode_count = n_wide;
+    s->dev.n_fnodes = (uint32_t)n_wide;
     s->dev.fnodes = (const float4 *)s->fnodes.ptr;
     s->dev.ftris = (const float4 *)s->ftris.ptr;
     return MRT_OK;

@@ -18,17 +18,13 @@ namespace mrt {
 
 constexpr float kEpsilon = 1.0e-06f;        // Utils.hpp:37
 constexpr float kRayLengthMax = 1.0e+30f;   // Utils.hpp:33
-constexpr int kWide = 4;                    // children per node of the FAST tree
-constexpr uint32_t kNodeNone = 0xFFFFFFFFu;
-// a child or stack entry of the FAST tree: a node index, or a leaf as kLeafCode | (count - 1) << 27 | first
-constexpr uint32_t kLeafCode = 0x80000000u;
-constexpr uint32_t kMaxLeafFirst = 1u << 27;
+constexpr int kWide = 8;                    // children per node of the FAST tree
+constexpr int kNodeWords = 32;              // 32-bit words per node of the FAST tree (128 bytes)
+constexpr uint32_t kMaxLeafTris = 3;        // triangles per leaf child of the FAST tree
+constexpr uint32_t kMaxFastTris = 1u << 27; // triangles of one FAST tree (indices and counts stay in 32 bits)
 constexpr float kSphereEpsilon = 1.0e-05f;  // Sphere.cpp:43,50
 
 #define MRT_HD __host__ __device__ __forceinline__
-MRT_HD uint32_t leaf_code(uint32_t first, uint32_t count) { return kLeafCode | ((count - 1u) << 27) | first; }
-MRT_HD uint32_t code_first(uint32_t c) { return c & (kMaxLeafFirst - 1u); }
-MRT_HD uint32_t code_count(uint32_t c) { return ((c >> 27) & 15u) + 1u; }
 
 struct V3 {
     float x, y, z;
@@ -144,9 +140,9 @@ struct DevScene {
     // accelerators
     int32_t accel;
     int32_t bvh_mode;
-    const float4 *fnodes;  // FAST BVH: kWide records of 2 float4 (min.xyz|a, max.xyz|b) per node
+    const float4 *fnodes;  // FAST BVH: 8-wide quantised nodes of 128 bytes (layout in mrt_trace.cuh)
     const float4 *ftris;   // FAST BVH: 3 float4 per triangle in leaf order (A|index, AB, AC)
-    uint32_t n_fnodes;     // records in fnodes (bounds of every node index read)
+    uint32_t n_fnodes;     // nodes in fnodes (bounds of every node index read)
     const RefNode *rnodes[3];
     uint32_t rnode_count[3];
     DevGrid grid[3];

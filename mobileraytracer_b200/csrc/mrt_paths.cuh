@@ -159,31 +159,6 @@ __device__ __forceinline__ bool path_next(const DevScene &s, const RenderParams 
     return false;
 }
 
-// any-hit leaf step on the closest-hit traversal state (best_t holds the shadow distance; the
-// first occluder ends the query), Shader::shadowTrace (Shader.cpp:162-187)
-template <class S>
-__device__ __forceinline__ void occ_leaf_on_trav(const S &s, const Ray &r, FastTrav &t) {
-    for (int q = 0; q < 2; ++q) {
-        const uint32_t first = q == 0 ? t.leaf_first : t.leaf2_first, count = q == 0 ? t.leaf_count : t.leaf2_count;
-        if (count == 0) continue;
-        if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); break; }
-        for (uint32_t k = first; k < first + count; ++k) {
-            const float4 A = __ldg(&s.ftris[3 * k]);
-            const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-            const float4 AC = __ldg(&s.ftris[3 * k + 2]);
-            if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
-            if (tri_occ(v3(A), v3(AB), v3(AC), r, t.best_t)) {
-                t.have = true;
-                t.node = kNodeNone;
-                t.sp = 0;
-                t.leaf_count = t.leaf2_count = 0;
-                return;
-            }
-        }
-    }
-    t.leaf_count = t.leaf2_count = 0;
-}
-
 // Work provides: total(), counter(), scene(lane), view(lane), params(lane),
 //   begin(item, lane, r): the path's camera ray (the lane's frames reset, root frame pushed),
 //   deliver(lane, rgb, flag): the path's value.
@@ -210,7 +185,7 @@ __device__ void persistent_paths(Work &work) {
             trav_begin<false>(s, r, dist, t);
             if (naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist)) {
                 t.have = true;
-                t.node = kNodeNone;
+                trav_clear(t);
             }
         } else {
             ++lane.n_closest;
@@ -248,12 +223,12 @@ __device__ void persistent_paths(Work &work) {
         // 2. node phase
         for (;;) {   // lanes holding a leaf step on speculatively while others search
             const bool w = active && trav_wants_node(t);
-            if (node_phase_over(w, active && t.leaf_count > 0)) break;
-            if (w || (active && trav_can_speculate(t))) trav_node_step<false>(work.view(lane), t, stk);
+            if (node_phase_over(w, active && trav_has_leaf(t))) break;
+            if (w || (active && trav_can_speculate(t))) trav_node_step<false>(work.view(lane), r, t, stk);
         }
-        // 3. leaf phase
-        if (active && t.leaf_count > 0) {
-            if (any) occ_leaf_on_trav(work.view(lane), r, t);
+        // 3. leaf phase (an any-hit query ends at its first occluder)
+        if (active && trav_has_leaf(t)) {
+            if (any) trav_occ_leaf_step(work.view(lane), r, t);
             else trav_leaf_step<false>(work.view(lane), r, t);
         }
         // 4. completion: the answer moves the path on.  Lanes whose query is answered wait until

@@ -133,7 +133,13 @@ struct NsWork {
     }
 };
 
-__global__ void __launch_bounds__(128, 8) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
+// resident blocks of 128 threads per SM for the NoShadows kernel (registers per thread: 65536 / (128 x this))
+#ifndef MRT_NS_BLOCKS_PER_SM
+#define MRT_NS_BLOCKS_PER_SM 8
+#endif
+constexpr int kNsBlocksPerSm = MRT_NS_BLOCKS_PER_SM;
+
+__global__ void __launch_bounds__(128, kNsBlocksPerSm) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
                                                                uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
@@ -655,7 +661,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             if (s->stop.load()) return cancelled(ctx, q);
             if (fast) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
-                k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
+                k_render_noshadows_fast<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
             } else if (accel == MRT_ACCEL_REGULAR_GRID) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
@@ -962,7 +968,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
         if (accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST) {
             const uint32_t tiles_x = o->width / 2u;   // width is a multiple of 16, rows of 16
             cudaMemsetAsync(counters, 0, sizeof(uint32_t), q);
-            k_render_noshadows_fast<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, 0u, p.n_tasks, counters, tiles_x);
+            k_render_noshadows_fast<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, p, 0u, p.n_tasks, counters, tiles_x);
         } else {
             MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, 0u, p.n_tasks, grid, q);
         }

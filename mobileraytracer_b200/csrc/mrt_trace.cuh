@@ -6,16 +6,15 @@
 // keep that order and those comparisons:
 //   * NAIVE, REGULAR_GRID and BVH/REFERENCE walk the reference structures in the reference order
 //     with the reference box test, so the result is the reference's bit for bit;
-//   * BVH/FAST walks a 4-wide tree (a Morton-ordered binary tree collapsed on the device) front to
-//     back with a conservative box test and keeps the lexicographic minimum (t, index): the
-//     Naive<T> result without visiting every triangle.
+//   * BVH/FAST walks an 8-wide tree with quantised child boxes (a Morton-ordered binary tree
+//     collapsed and compressed on the device) nearest child first with a conservative box test and
+//     keeps the lexicographic minimum (t, index): the Naive<T> result without visiting every triangle.
 #pragma once
 
 #include "mrt_device.cuh"
 
 namespace mrt {
 
-constexpr int kFastStack = 128;           // entries of the FAST traversal stack (3 pushes per node at most)
 constexpr int kRefStack = 128;
 constexpr uint32_t kMaxGridSteps = 1u << 20;
 constexpr uint32_t kMaxBvhSteps = 1u << 24;   // traversal iterations per ray before MRT_ERR_LIMIT
@@ -340,25 +339,41 @@ __device__ bool grid_occ(const DevScene &s, const Ray &r, float dist) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// FAST BVH: Morton-ordered binary tree, child pairs adjacent (64 B per pair), triangles in leaf
-// order as 48-byte records.  Conservative slab test against padded boxes; front-to-back order
-// with the entry distance kept on the stack.
+// FAST BVH: 8-wide nodes of 128 bytes with 16-bit quantised child boxes, one node per traversal
+// step.  A node's internal children are stored contiguously from its child base (in slot order), the
+// triangles of its leaf children contiguously from its triangle base (48-byte records A|index, AB,
+// AC).  The compressed wide node and its traversal by node groups (a base index and a bit mask of the
+// children still to visit, one stack entry per node instead of one per child) follow Ylitie, Karras
+// and Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017);
+// here the boxes are quantised to 16 bits and every plane distance is bounded by directed rounding.
+//
+// Node, 32 words (the fnodes array holds n_fnodes of them):
+//   w[0..2]  origin p of the quantisation grid (floats)
+//   w[3]     ex | ey << 8 | ez << 16 (axis a's grid step is 2^(e_a - 127)) | imask << 24 (slots
+//            holding internal children)
+//   w[4]     child base: node index of the first internal child
+//   w[5]     triangle base: record index of the first triangle of the leaf children
+//   w[6..7]  one byte per slot: a leaf child's triangle bits (1, 3 or 7 for 1..3 triangles) << 5 | the
+//            offset of its first triangle from the triangle base; 0 for internal and empty slots
+//   w[8+k], w[16+k], w[24+k]   slot k's box on x, y, z: qlo | qhi << 16, the planes p + step * q;
+//            the quantised box contains the exact box of everything below the slot
+// Slots are assigned by the octant of the child's centre within the node, so visiting the children
+// in the order slot ^ octant(ray direction) is close to front to back.
 // ---------------------------------------------------------------------------------------------
-// A ray prepared for the conservative box test of the FAST tree.  The plane distances are computed
-// as fma(plane, inv, -c) with c = o * inv moved outward by a margin (2^-20 |o * inv|, more than the
-// rounding of o * inv and of the shift itself), so the entry distance is never overestimated and the
-// exit distance never underestimated; the remaining rounding is relative and covered by the 1e-6
-// tolerance of the comparison.  The test may therefore accept a box the ray misses, never reject one
-// it touches.
+
+// A ray prepared for the quantised box test: 1/d (components of |d| < 1e-20 replaced by +-1e-20) and
+// the octant of the direction.  With A = step * (1/d) (exact: a power of two times a float) the
+// distance of plane p + step * q is (p - o) / d + q * A; the entry distance is computed rounded down
+// from a lower bound of (p - o) / d (built from o * (1/d) rounded up), the exit distance rounded up
+// from an upper bound, so with respect to the rounded 1/d the test never rejects a box the ray
+// touches.  The rounding of 1/d itself is relative and covered by the 1e-6 tolerance of the
+// comparison.  The grid offset q enters as the float 2^23 + q (built by one byte permute) with
+// 2^23 * A folded into the bound, which loosens a plane by at most one grid step (1/65535 of the
+// node's extent).
 struct FastRay {
     V3 inv;
-    V3 clo, chi;   // offsets of the lo and hi planes
+    uint32_t oct;    // bit a: the direction is negative along axis a
 };
-
-__device__ __forceinline__ float fast_shift(float p, bool up) {
-    const float m = fabsf(p) * 0x1p-20f;
-    return up ? p + m : p - m;
-}
 
 __device__ __forceinline__ FastRay fast_ray(const Ray &r) {
     FastRay f;
@@ -367,37 +382,94 @@ __device__ __forceinline__ FastRay fast_ray(const Ray &r) {
     const float dy = fabsf(r.d.y) < e ? copysignf(e, r.d.y) : r.d.y;
     const float dz = fabsf(r.d.z) < e ? copysignf(e, r.d.z) : r.d.z;
     f.inv = V3{1.0f / dx, 1.0f / dy, 1.0f / dz};
-    const float px = r.o.x * f.inv.x, py = r.o.y * f.inv.y, pz = r.o.z * f.inv.z;
-    // the lo plane is the entry plane when inv >= 0: its offset moves up (distance down)
-    f.clo = V3{fast_shift(px, f.inv.x >= 0.0f), fast_shift(py, f.inv.y >= 0.0f), fast_shift(pz, f.inv.z >= 0.0f)};
-    f.chi = V3{fast_shift(px, f.inv.x < 0.0f), fast_shift(py, f.inv.y < 0.0f), fast_shift(pz, f.inv.z < 0.0f)};
+    f.oct = (f.inv.x < 0.0f ? 1u : 0u) | (f.inv.y < 0.0f ? 2u : 0u) | (f.inv.z < 0.0f ? 4u : 0u);
     return f;
 }
 
-// true when the ray segment [0, tmax] may touch the box; tnear = entry distance (a lower bound)
-__device__ __forceinline__ bool fast_slab(float4 lo, float4 hi, const FastRay &f, float tmax, float &tnear) {
-    const float x1 = __fmaf_rn(lo.x, f.inv.x, -f.clo.x), x2 = __fmaf_rn(hi.x, f.inv.x, -f.chi.x);
-    const float y1 = __fmaf_rn(lo.y, f.inv.y, -f.clo.y), y2 = __fmaf_rn(hi.y, f.inv.y, -f.chi.y);
-    const float z1 = __fmaf_rn(lo.z, f.inv.z, -f.clo.z), z2 = __fmaf_rn(hi.z, f.inv.z, -f.chi.z);
-    const float tn = fmaxf(fmaxf(fminf(x1, x2), fminf(y1, y2)), fmaxf(fminf(z1, z2), 0.0f));
-    const float tf = fminf(fminf(fmaxf(x1, x2), fmaxf(y1, y2)), fminf(fmaxf(z1, z2), tmax));
-    tnear = tn;
-    return tn <= tf * 1.000001f;
-}
-
 struct FastCounts {
-    uint32_t nodes;  // 32-byte node records fetched
+    uint32_t nodes;  // 128-byte nodes fetched
     uint32_t tris;   // 48-byte triangle records fetched
 };
 
+// the children of one node that the ray segment [0, tmax] may touch
+struct NodeHits {
+    uint32_t child_base;   // node index of the node's first internal child
+    uint32_t groups;       // imask << 8 | internal children hit, bit (slot ^ ray octant)
+    uint32_t tri_base;     // record index of the node's first leaf triangle
+    uint32_t tris;         // leaf triangles hit: bit j is record tri_base + j
+};
+
+__device__ __forceinline__ uint32_t uint4_word(const uint4 &a, int k) {
+    switch (k & 3) {
+        case 0: return a.x; case 1: return a.y; case 2: return a.z; default: return a.w;
+    }
+}
+
+// 2^23 + (lo or hi half of w) as a float: byte permute of w with 0x4B000000 (selector 0x7410 takes
+// the low half, 0x7432 the high half)
+__device__ __forceinline__ float grid_offset(uint32_t w, uint32_t sel) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, sel));
+}
+
+template <class S>
+__device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const FastRay &f, const V3 &o, float tmax) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(s.fnodes) + (size_t)node * (kNodeWords / 4);
+    const uint4 h0 = __ldg(p), h1 = __ldg(p + 1);
+    // per axis: A = step / d, and bounds of (p - o) / d - 2^23 A
+    const float ax = __uint_as_float((h0.w & 0xFFu) << 23) * f.inv.x;
+    const float ay = __uint_as_float(((h0.w >> 8) & 0xFFu) << 23) * f.inv.y;
+    const float az = __uint_as_float(((h0.w >> 16) & 0xFFu) << 23) * f.inv.z;
+    const float lox = __fmaf_rd(-8388608.0f, ax, __fmaf_rd(__uint_as_float(h0.x), f.inv.x, -__fmul_ru(o.x, f.inv.x)));
+    const float loy = __fmaf_rd(-8388608.0f, ay, __fmaf_rd(__uint_as_float(h0.y), f.inv.y, -__fmul_ru(o.y, f.inv.y)));
+    const float loz = __fmaf_rd(-8388608.0f, az, __fmaf_rd(__uint_as_float(h0.z), f.inv.z, -__fmul_ru(o.z, f.inv.z)));
+    const float hix = __fmaf_ru(-8388608.0f, ax, __fmaf_ru(__uint_as_float(h0.x), f.inv.x, -__fmul_rd(o.x, f.inv.x)));
+    const float hiy = __fmaf_ru(-8388608.0f, ay, __fmaf_ru(__uint_as_float(h0.y), f.inv.y, -__fmul_rd(o.y, f.inv.y)));
+    const float hiz = __fmaf_ru(-8388608.0f, az, __fmaf_ru(__uint_as_float(h0.z), f.inv.z, -__fmul_rd(o.z, f.inv.z)));
+    // the entry plane is the lo plane where the direction is positive
+    const uint32_t nx = 0x7410u + ((f.oct & 1u) ? 0x22u : 0u);
+    const uint32_t ny = 0x7410u + ((f.oct & 2u) ? 0x22u : 0u);
+    const uint32_t nz = 0x7410u + ((f.oct & 4u) ? 0x22u : 0u);
+    const uint32_t imask = h0.w >> 24;
+    uint32_t groups = 0, tris = 0;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {   // four children at a time: fewer registers live
+        const uint4 xq = __ldg(p + 2 + half), yq = __ldg(p + 4 + half), zq = __ldg(p + 6 + half);
+        const uint32_t meta4 = half ? h1.w : h1.z;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = 4 * half + j;
+            const uint32_t wx = uint4_word(xq, j), wy = uint4_word(yq, j), wz = uint4_word(zq, j);
+            const float tnx = __fmaf_rd(grid_offset(wx, nx), ax, lox), tfx = __fmaf_ru(grid_offset(wx, nx ^ 0x22u), ax, hix);
+            const float tny = __fmaf_rd(grid_offset(wy, ny), ay, loy), tfy = __fmaf_ru(grid_offset(wy, ny ^ 0x22u), ay, hiy);
+            const float tnz = __fmaf_rd(grid_offset(wz, nz), az, loz), tfz = __fmaf_ru(grid_offset(wz, nz ^ 0x22u), az, hiz);
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+            if (tn <= tf * 1.000001f) {
+                const uint32_t meta = (meta4 >> (8 * j)) & 0xFFu;
+                tris |= (meta >> 5) << (meta & 31u);
+                groups |= ((imask >> k) & 1u) << (k ^ f.oct);
+            }
+        }
+    }
+    return NodeHits{h1.x, (imask << 8) | groups, h1.y, tris};
+}
+
+// node index of the child at visiting key `key` of a group (child base, imask << 8 | ...)
+__device__ __forceinline__ uint32_t group_node(uint32_t base, uint32_t groups, uint32_t key, uint32_t oct) {
+    const uint32_t slot = key ^ oct;
+    return base + __popc((groups >> 8) & ((1u << slot) - 1u));
+}
+
 template <bool kCount, class S>
-__device__ __forceinline__ void fast_leaf(const S &s, const Ray &r, uint32_t first, uint32_t count,
-                                          float &best_t, uint32_t &best_i, bool &have, FastCounts &cnt) {
-    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
-    for (uint32_t k = first; k < first + count; ++k) {
-        const float4 A = __ldg(&s.ftris[3 * k]);
-        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+__device__ __forceinline__ void fast_tris(const S &s, const Ray &r, uint32_t base, uint32_t bits, float &best_t,
+                                          uint32_t &best_i, bool &have, FastCounts &cnt) {
+    while (bits) {
+        const uint32_t k = base + (uint32_t)(__ffs(bits) - 1);
+        bits &= bits - 1u;
+        if (k >= s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return; }
+        const float4 A = __ldg(&s.ftris[3 * (size_t)k]);
+        const float4 AB = __ldg(&s.ftris[3 * (size_t)k + 1]);
+        const float4 AC = __ldg(&s.ftris[3 * (size_t)k + 2]);
         if (kCount) cnt.tris++;
         const uint32_t idx = __float_as_uint(A.w);
         if (r.exclude == hid(MRT_PRIM_TRIANGLE, idx)) continue;
@@ -411,158 +483,175 @@ __device__ __forceinline__ void fast_leaf(const S &s, const Ray &r, uint32_t fir
     }
 }
 
-
-__device__ __forceinline__ void cmp_swap(float (&t)[kWide], uint32_t (&c)[kWide], int i, int j) {
-    const bool sw = t[j] < t[i];
-    const float ti = t[i], tj = t[j];
-    const uint32_t ci = c[i], cj = c[j];
-    t[i] = sw ? tj : ti;
-    t[j] = sw ? ti : tj;
-    c[i] = sw ? cj : ci;
-    c[j] = sw ? ci : cj;
-}
-
-// One node of the FAST tree: kWide child records {min.xyz, a}{max.xyz, b} (b = 0: internal child,
-// node a; b > 0: leaf of b triangles, a = its leaf code; b < 0: empty slot).  Returns the number of children the
-// ray segment [0, tmax] may touch; with kSort their (entry distance, code) come first, nearest
-// first, the others follow at +inf.
-template <bool kSort, class S>
-__device__ __forceinline__ int wide_children(const S &s, uint32_t node, const FastRay &f, float tmax,
-                                             float (&t)[kWide], uint32_t (&c)[kWide]) {
-    const float4 *p = s.fnodes + (size_t)node * (2 * kWide);
-    float4 lo[kWide], hi[kWide];
-#pragma unroll
-    for (int k = 0; k < kWide; ++k) {
-        lo[k] = __ldg(p + 2 * k);
-        hi[k] = __ldg(p + 2 * k + 1);
-    }
-    int n = 0;
-#pragma unroll
-    for (int k = 0; k < kWide; ++k) {
-        const int b = __float_as_int(hi[k].w);
-        float tn;
-        const bool hit = fast_slab(lo[k], hi[k], f, tmax, tn) && b >= 0;
-        t[k] = hit ? tn : __int_as_float(0x7f800000);
-        c[k] = __float_as_uint(lo[k].w);   // node index, or the leaf code written by the build
-        n += hit ? 1 : 0;
-    }
-    if (kSort) {
-        static_assert(kWide == 4, "sorting network for 4 children");
-        cmp_swap(t, c, 0, 1);
-        cmp_swap(t, c, 2, 3);
-        cmp_swap(t, c, 0, 2);
-        cmp_swap(t, c, 1, 3);
-        cmp_swap(t, c, 1, 2);
-    } else {
-        // compact the hits to the front, order kept
-#pragma unroll
-        for (int k = 1; k < kWide; ++k)
-#pragma unroll
-            for (int m = k; m > 0; --m)
-                if (t[m - 1] == __int_as_float(0x7f800000) && t[m] != __int_as_float(0x7f800000)) {
-                    t[m - 1] = t[m]; t[m] = __int_as_float(0x7f800000);
-                    const uint32_t x = c[m - 1]; c[m - 1] = c[m]; c[m] = x;
-                }
-    }
-    return n;
-}
-
 template <class S>
-__device__ __forceinline__ bool node_in_range(const S &s, uint32_t node) {
-    return (uint64_t)(node + 1u) * kWide <= (uint64_t)s.n_fnodes;
-}
-
-// closest triangle with the reference's accept rule against the incoming length `len`: front to
-// back, leaves as they are reached, entries beyond the best distance culled when popped
-template <bool kCount = false>
-__device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t &id, FastCounts *counts = nullptr) {
-    if (s.n_tri == 0) return false;
-    FastCounts cnt{0, 0};
-    const FastRay f = fast_ray(r);
-    float best_t = len;
-    uint32_t best_i = 0;   // ties with a plane/sphere distance never win (index < 0 is impossible)
-    bool have = false;
-    uint32_t stack_n[kFastStack];
-    float stack_t[kFastStack];
-    int sp = 0;
-    uint32_t cur = 0;      // the root node
-    uint32_t steps = 0;
-    for (;;) {
-        if (cur == kNodeNone) {
-            bool found = false;
-            while (sp > 0) {
-                --sp;
-                if (stack_t[sp] <= best_t * 1.000001f) { cur = stack_n[sp]; found = true; break; }
-            }
-            if (!found) break;
-        } else if (cur & kLeafCode) {
-            fast_leaf<kCount>(s, r, code_first(cur), code_count(cur), best_t, best_i, have, cnt);
-            cur = kNodeNone;
-        } else {
-            if (!node_in_range(s, cur) || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); break; }
-            float ct[kWide];
-            uint32_t cc[kWide];
-            const int n = wide_children<true>(s, cur, f, best_t, ct, cc);
-            if (kCount) cnt.nodes += kWide;
-            cur = kNodeNone;
-            if (n > 0) {
-                if (sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); break; }
-#pragma unroll
-                for (int k = kWide - 1; k >= 1; --k)
-                    if (k < n) { stack_n[sp] = cc[k]; stack_t[sp] = ct[k]; ++sp; }
-                cur = cc[0];
-            }
-        }
-    }
-    if (counts) *counts = cnt;
-    if (!have) return false;
-    len = best_t;
-    id = hid(MRT_PRIM_TRIANGLE, best_i);
-    return true;
-}
-
-__device__ __forceinline__ bool fast_occ_leaf(const DevScene &s, const Ray &r, uint32_t first, uint32_t count,
-                                              float dist) {
-    if (first + count > s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return false; }
-    for (uint32_t k = first; k < first + count; ++k) {
-        const float4 A = __ldg(&s.ftris[3 * k]);
-        const float4 AB = __ldg(&s.ftris[3 * k + 1]);
-        const float4 AC = __ldg(&s.ftris[3 * k + 2]);
+__device__ __forceinline__ bool fast_tris_occ(const S &s, const Ray &r, uint32_t base, uint32_t bits, float dist) {
+    while (bits) {
+        const uint32_t k = base + (uint32_t)(__ffs(bits) - 1);
+        bits &= bits - 1u;
+        if (k >= s.n_tri) { raise_error(s, MRT_ERR_LIMIT); return false; }
+        const float4 A = __ldg(&s.ftris[3 * (size_t)k]);
+        const float4 AB = __ldg(&s.ftris[3 * (size_t)k + 1]);
+        const float4 AC = __ldg(&s.ftris[3 * (size_t)k + 2]);
         if (r.exclude == hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w))) continue;
         if (tri_occ(v3(A), v3(AB), v3(AC), r, dist)) return true;
     }
     return false;
 }
 
-__device__ inline bool fast_occ(const DevScene &s, const Ray &r, float dist) {
+// ---------------------------------------------------------------------------------------------
+// resumable traversal state of one ray (closest hit; any hit keeps best_t = the shadow distance and
+// sets `have` at the first occluder).  The stack holds node groups, at most one per tree level.
+// ---------------------------------------------------------------------------------------------
+constexpr int kFastStack = 64;   // the tree is at most 62 levels deep (30-bit Morton codes + 32 index bits)
+
+struct FastTrav {
+    FastRay f;
+    float best_t;
+    uint32_t best_i;
+    uint32_t g_base, g_bits;     // node group being expanded: child base, imask << 8 | keys left
+    uint32_t t_base, t_bits;     // triangles waiting for the leaf phase
+    uint32_t t2_base, t2_bits;   // a second group of them, found while the warp still searched
+    int sp;
+    bool have;
+    uint32_t c_nodes, c_tris;
+};
+
+struct TravStack {
+    uint2 e[kFastStack];
+};
+
+template <bool kCount, class S>
+__device__ __forceinline__ void trav_begin(const S &s, const Ray &r, float len0, FastTrav &t) {
+    t.f = fast_ray(r);
+    t.best_t = len0;
+    t.best_i = 0;   // ties with a plane/sphere distance never win (index < 0 is impossible)
+    t.have = false;
+    t.g_base = 0;
+    // the root as the only internal child (slot 0) of a virtual group
+    t.g_bits = s.n_tri == 0 ? 0u : ((1u << 8) | (1u << t.f.oct));
+    t.t_bits = 0;
+    t.t2_bits = 0;
+    t.sp = 0;
+    t.c_nodes = 0;
+    t.c_tris = 0;
+}
+
+__device__ __forceinline__ bool trav_has_nodes(const FastTrav &t) { return (t.g_bits & 0xFFu) != 0u || t.sp > 0; }
+__device__ __forceinline__ bool trav_has_leaf(const FastTrav &t) { return t.t_bits != 0u; }
+__device__ __forceinline__ bool trav_wants_node(const FastTrav &t) { return t.t_bits == 0u && trav_has_nodes(t); }
+// a lane with triangles waiting may go on with node steps while others of its warp still search
+// (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs", HPG 2009: speculative
+// traversal), up to a second group of triangles
+__device__ __forceinline__ bool trav_can_speculate(const FastTrav &t) {
+    return t.t_bits != 0u && t.t2_bits == 0u && trav_has_nodes(t);
+}
+__device__ __forceinline__ bool trav_finished(const FastTrav &t) {
+    return t.t_bits == 0u && t.t2_bits == 0u && !trav_has_nodes(t);
+}
+// nothing left to do (an error, or the first occluder of an any-hit query)
+__device__ __forceinline__ void trav_clear(FastTrav &t) {
+    t.g_bits = 0;
+    t.sp = 0;
+    t.t_bits = 0;
+    t.t2_bits = 0;
+}
+
+template <class S>
+__device__ __forceinline__ bool node_in_range(const S &s, uint32_t node) {
+    return node < s.n_fnodes;
+}
+
+// one node step: the next child of the current group (a group popped first when it is empty), its
+// node tested, its hit internal children becoming the current group (the rest of the old one pushed)
+template <bool kCount, class S>
+__device__ __forceinline__ void trav_node_step(const S &s, const Ray &r, FastTrav &t, TravStack &st) {
+    if ((t.g_bits & 0xFFu) == 0u) {
+        if (t.sp == 0) return;
+        const uint2 e = st.e[--t.sp];
+        t.g_base = e.x;
+        t.g_bits = e.y;
+    }
+    const uint32_t key = (uint32_t)(__ffs(t.g_bits & 0xFFu) - 1);
+    t.g_bits &= ~(1u << key);
+    const uint32_t node = group_node(t.g_base, t.g_bits, key, t.f.oct);
+    if (t.g_bits & 0xFFu) {
+        if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); trav_clear(t); return; }
+        st.e[t.sp++] = make_uint2(t.g_base, t.g_bits);
+    }
+    if (!node_in_range(s, node)) { raise_error(s, MRT_ERR_LIMIT); trav_clear(t); return; }
+    const NodeHits h = node_hits(s, node, t.f, r.o, t.best_t);
+    if (kCount) t.c_nodes++;
+    t.g_base = h.child_base;
+    t.g_bits = h.groups;
+    if (h.tris) {
+        if (t.t_bits == 0u) { t.t_base = h.tri_base; t.t_bits = h.tris; }
+        else { t.t2_base = h.tri_base; t.t2_bits = h.tris; }
+    }
+}
+
+template <bool kCount, class S>
+__device__ __forceinline__ void trav_leaf_step(const S &s, const Ray &r, FastTrav &t) {
+    FastCounts cnt{0, 0};
+    fast_tris<kCount>(s, r, t.t_base, t.t_bits, t.best_t, t.best_i, t.have, cnt);
+    if (t.t2_bits) fast_tris<kCount>(s, r, t.t2_base, t.t2_bits, t.best_t, t.best_i, t.have, cnt);
+    if (kCount) t.c_tris += cnt.tris;
+    t.t_bits = 0;
+    t.t2_bits = 0;
+}
+
+// any-hit leaf step on the same state (best_t holds the shadow distance): the first occluder ends
+// the query with `have` set
+template <class S>
+__device__ __forceinline__ void trav_occ_leaf_step(const S &s, const Ray &r, FastTrav &t) {
+    if (fast_tris_occ(s, r, t.t_base, t.t_bits, t.best_t) ||
+        (t.t2_bits && fast_tris_occ(s, r, t.t2_base, t.t2_bits, t.best_t))) {
+        t.have = true;
+        trav_clear(t);
+        return;
+    }
+    t.t_bits = 0;
+    t.t2_bits = 0;
+}
+
+// closest triangle with the reference's accept rule against the incoming length `len` (one ray per
+// thread): lexicographic minimum (t, index) over the triangles of every box the ray may touch
+template <bool kCount = false>
+__device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t &id, FastCounts *counts = nullptr) {
     if (s.n_tri == 0) return false;
-    const FastRay f = fast_ray(r);
-    uint32_t stack_n[kFastStack];
-    int sp = 0;
-    uint32_t cur = 0;
+    FastTrav t;
+    TravStack st;
+    trav_begin<kCount>(s, r, len, t);
     uint32_t steps = 0;
-    for (;;) {
-        if (cur == kNodeNone) {
-            if (sp == 0) return false;
-            cur = stack_n[--sp];
-        } else if (cur & kLeafCode) {
-            if (fast_occ_leaf(s, r, code_first(cur), code_count(cur), dist)) return true;
-            cur = kNodeNone;
+    while (!trav_finished(t)) {
+        if (trav_has_leaf(t)) {
+            trav_leaf_step<kCount>(s, r, t);
         } else {
-            if (!node_in_range(s, cur) || ++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); return false; }
-            float ct[kWide];
-            uint32_t cc[kWide];
-            const int n = wide_children<false>(s, cur, f, dist, ct, cc);
-            cur = kNodeNone;
-            if (n > 0) {
-                if (sp + n - 1 > kFastStack) { raise_error(s, MRT_ERR_LIMIT); return false; }
-#pragma unroll
-                for (int k = kWide - 1; k >= 1; --k)
-                    if (k < n) stack_n[sp++] = cc[k];
-                cur = cc[0];
-            }
+            if (++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); break; }
+            trav_node_step<kCount>(s, r, t, st);
         }
     }
+    if (counts) *counts = FastCounts{t.c_nodes, t.c_tris};
+    if (!t.have) return false;
+    len = t.best_t;
+    id = hid(MRT_PRIM_TRIANGLE, t.best_i);
+    return true;
+}
+
+__device__ inline bool fast_occ(const DevScene &s, const Ray &r, float dist) {
+    if (s.n_tri == 0) return false;
+    FastTrav t;
+    TravStack st;
+    trav_begin<false>(s, r, dist, t);
+    uint32_t steps = 0;
+    while (!trav_finished(t)) {
+        if (trav_has_leaf(t)) {
+            trav_occ_leaf_step(s, r, t);
+        } else {
+            if (++steps > kMaxBvhSteps) { raise_error(s, MRT_ERR_LIMIT); return false; }
+            trav_node_step<false>(s, r, t, st);
+        }
+    }
+    return t.have;
 }
 
 // ---------------------------------------------------------------------------------------------
