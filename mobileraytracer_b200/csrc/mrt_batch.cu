@@ -264,6 +264,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_shadow(BatchSta
 __device__ __forceinline__ void shade_direct_node(const DevScene &s, const RenderParams &p, const RayRec &rr,
                                                      uint32_t hit_id, float hit_t, const Stream &st, ShadeLane &o) {
     o.n_child = 0;
+    o.child_mask = 0;
     o.n_shadow = 0;
     o.shaded = false;
     NodeRec &nd = o.nd;
@@ -297,6 +298,7 @@ __global__ void __launch_bounds__(128) k_batch_shade(BatchState b, int level) {
         const uint32_t idx = L.start + (active ? i : 0);
         ShadeLane o;
         o.n_child = 0;
+        o.child_mask = 0;
         o.n_shadow = 0;
         o.shaded = false;
         RayRec rr;
@@ -311,13 +313,13 @@ __global__ void __launch_bounds__(128) k_batch_shade(BatchState b, int level) {
             const NodeRec &in = b.nodes[idx];
             if (direct_shader(p.shader)) shade_direct_node(s, p, rr, in.hit_id, in.hit_t, st, o);
             else shade_ray(s, p, rr, in.hit_id, in.hit_t, st, o);
-            b.nodes[idx] = o.nd;
+            store_node(b.nodes[idx], o.nd);
         }
         const uint32_t cbase = warp_alloc(o.n_child, &next->count);
         const uint32_t sbase = warp_alloc(o.n_shadow, &b.levels[level].shadow_count);
         if (!active) continue;
         const DevScene &s = b.scenes[job];
-        emit_children(s, o, rr, idx, next_start + cbase, b.rays, b.ray_cap);
+        emit_children(s, o, rr, st, idx, next_start + cbase, b.rays, b.ray_cap);
         emit_shadows(s, b.jobs[job], st, o, rr, idx, sbase, b.shadows, b.shadow_cap);
     }
 }
@@ -328,14 +330,20 @@ __global__ void __launch_bounds__(128) k_batch_resolve(BatchState b, int level) 
     L.count = min(L.count, b.ray_cap - L.start);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
         const uint32_t idx = L.start + i;
-        const NodeRec nd = b.nodes[idx];
-        const RayRec rr = b.rays[idx];
-        const uint32_t job = b.root_job[rr.root];
-        const RenderParams &p = b.jobs[job];
-        const Stream st = stream_of(p, b.root_local[rr.root]);
-        V3 rgb;
-        bool flag;
-        resolve_node(b.scenes[job], p, nd, rr, st, rgb, flag);
+        const NodeRec &nd = b.nodes[idx];
+        const RayRec &rr = b.rays[idx];
+        V3 rgb{0.0f, 0.0f, 0.0f};
+        bool flag = false;
+        const uint32_t kind = nd.flags & 3u;
+        if (kind == kEmit) {
+            rgb = nd.point;
+            flag = true;
+        } else if (kind == kShaded) {   // misses and cut nodes are black
+            const uint32_t job = b.root_job[rr.root];
+            const RenderParams &p = b.jobs[job];
+            const Stream st = stream_of(p, b.root_local[rr.root]);
+            resolve_node(b.scenes[job], p, nd, rr, st, rgb, flag);
+        }
         if (rr.parent == 0xFFFFFFFFu) {
             b.root_rgb[rr.root] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
         } else {

@@ -451,6 +451,36 @@ struct CollapseItem {
 
 __device__ __forceinline__ bool rec_internal(const float4 *bin, uint32_t r) { return __float_as_int(bin[2 * (size_t)r + 1].w) == 0; }
 
+#ifndef MRT_COLLAPSE_SMALL
+#define MRT_COLLAPSE_SMALL 1
+#endif
+// The triangles below internal record r when they are at most kMaxLeafTris (a subtree's triangles
+// are contiguous in Morton order): a full wide node keeps such a child as one leaf instead of
+// spending a 128-byte node on two or three children.
+__device__ __forceinline__ bool small_subtree(const float4 *bin, uint32_t n_records, uint32_t r, uint32_t &first,
+                                             uint32_t &count) {
+    uint32_t st[kMaxLeafTris + 1];
+    int sp = 0;
+    st[sp++] = r;
+    count = 0;
+    while (sp > 0) {
+        const uint32_t x = st[--sp];
+        if (rec_internal(bin, x)) {
+            const uint32_t a = __float_as_uint(bin[2 * (size_t)x].w);
+            if (a < 2u || (uint64_t)a + 1u >= n_records || sp + 2 > kMaxLeafTris + 1) return false;
+            st[sp++] = a + 1u;   // the left child is taken first: triangles in Morton order
+            st[sp++] = a;
+        } else {
+            const uint32_t f = __float_as_uint(bin[2 * (size_t)x].w), c = (uint32_t)__float_as_int(bin[2 * (size_t)x + 1].w);
+            if (count == 0) first = f;
+            else if (f != first + count) return false;
+            count += c;
+            if (count > kMaxLeafTris) return false;
+        }
+    }
+    return count > 0;
+}
+
 // grid step exponent E of one axis (2^E >= extent / 65534)
 __device__ __forceinline__ int grid_exponent(float lo, float hi) {
     const double want = ((double)hi - (double)lo) / 65534.0;
@@ -504,6 +534,17 @@ __global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, c
         nlo = make_float4(fminf(nlo.x, lo[k].x), fminf(nlo.y, lo[k].y), fminf(nlo.z, lo[k].z), 0.0f);
         nhi = make_float4(fmaxf(nhi.x, hi[k].x), fmaxf(nhi.y, hi[k].y), fmaxf(nhi.z, hi[k].z), 0.0f);
     }
+    // internal children left over (the node is full): small ones become leaves
+    bool internal[kWide];
+    for (int k = 0; k < m; ++k) {
+        internal[k] = rec_internal(bin, rec[k]);
+        uint32_t f = 0, c = 0;
+        if (MRT_COLLAPSE_SMALL && internal[k] && small_subtree(bin, n_records, rec[k], f, c)) {
+            internal[k] = false;
+            lo[k].w = __uint_as_float(f);
+            hi[k].w = __int_as_float((int)c);
+        }
+    }
     // slots by octant: the child whose centre lies on the high side of axis a prefers slots with bit a set
     const float cx = 0.5f * (nlo.x + nhi.x), cy = 0.5f * (nlo.y + nhi.y), cz = 0.5f * (nlo.z + nhi.z);
     int slot_of[kWide];
@@ -535,7 +576,7 @@ __global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, c
     uint32_t imask = 0, n_int = 0, n_lt = 0;
     for (int k = 0; k < m; ++k) {
         child_at[slot_of[k]] = k;
-        if (rec_internal(bin, rec[k])) { imask |= 1u << slot_of[k]; ++n_int; }
+        if (internal[k]) { imask |= 1u << slot_of[k]; ++n_int; }
         else n_lt += (uint32_t)__float_as_int(hi[k].w);
     }
     const uint32_t child_base = n_int ? atomicAdd(&ctrs[1], n_int) : 0u;

@@ -80,6 +80,7 @@ __device__ __forceinline__ void path_shade(const DevScene &s, const RenderParams
     if (direct_shader(p.shader)) {
         // NoShadows / DepthMap / DiffuseMaterial: the value is final at the camera ray
         o.n_child = 0;
+        o.child_mask = 0;
         o.shaded = false;
         NodeRec &nd = o.nd;
         nd.flags = kMiss;
@@ -101,9 +102,11 @@ __device__ __forceinline__ void path_shade(const DevScene &s, const RenderParams
     f.n_child = (uint8_t)o.n_child;
     f.next_child = 0;
     f.next_j = 0;
-    for (uint32_t c = 0; c < o.n_child; ++c) {
-        f.child_d[c] = o.child[c].d;
-        f.child_slot[c] = (uint8_t)o.child_slot[c];
+    uint32_t c = 0;
+    for (uint32_t m = o.child_mask; m; m &= m - 1u, ++c) {
+        const uint32_t slot = (uint32_t)(__ffs(m) - 1);
+        f.child_d[c] = child_dir(o, r.d, L.st, f.code, slot);
+        f.child_slot[c] = (uint8_t)slot;
     }
 }
 
@@ -177,23 +180,21 @@ __device__ void persistent_paths(Work &work) {
     bool any = false;
     FastTrav t;
     TravStack stk;
-    float len0 = kRayLengthMax;
-    uint32_t id0 = MRT_HIT_NONE;
     auto start = [&](const DevScene &s) {
         if (any) {
             ++lane.n_shadow;
-            trav_begin<false>(s, r, dist, t);
+            trav_begin<false>(s, r, dist, MRT_HIT_NONE, t);
             if (naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist)) {
-                t.have = true;
+                trav_set_occluded(t);
                 trav_clear(t);
             }
         } else {
             ++lane.n_closest;
-            len0 = kRayLengthMax;
-            id0 = MRT_HIT_NONE;
-            naive_trace<kPlane>(s, r, len0, id0);
-            naive_trace<kSphere>(s, r, len0, id0);
-            trav_begin<false>(s, r, len0, t);
+            float len = kRayLengthMax;
+            uint32_t id = MRT_HIT_NONE;
+            naive_trace<kPlane>(s, r, len, id);
+            naive_trace<kSphere>(s, r, len, id);
+            trav_begin<false>(s, r, len, id, t);
         }
     };
     for (;;) {
@@ -239,14 +240,13 @@ __device__ void persistent_paths(Work &work) {
             const DevScene &s = work.scene(lane);
             const RenderParams &p = work.params(lane);
             if (any) {
-                if (t.have) {
+                if (trav_hit(t)) {
                     PathFrame &f = lane.fr[lane.top - 1];
                     f.nd.occluded |= 1u << ((f.next_j - 1u) & 31u);
                 }
             } else {
-                float len = len0;
-                uint32_t id = id0;
-                if (t.have) { len = t.best_t; id = hid(MRT_PRIM_TRIANGLE, t.best_i); }
+                float len = t.best_t;
+                uint32_t id = t.best_id;
                 const bool hit_light = lights_trace(s, r, len, id);
                 const bool hit = id != MRT_HIT_NONE || hit_light;
                 path_shade(s, p, lane, r, hit ? id : MRT_HIT_NONE, len);

@@ -43,12 +43,12 @@ __device__ __forceinline__ bool node_phase_over(bool searching, bool holding_lea
 // (Shader.cpp:124-150), all with the reference accept rule.
 // ---------------------------------------------------------------------------------------------
 template <bool kCount, class Work, class Lane>
-__device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastTrav &t, float &len, uint32_t &id) {
-    len = kRayLengthMax;
-    id = MRT_HIT_NONE;
+__device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastTrav &t) {
+    float len = kRayLengthMax;
+    uint32_t id = MRT_HIT_NONE;
     naive_trace<kPlane>(s, r, len, id);
     naive_trace<kSphere>(s, r, len, id);
-    trav_begin<kCount>(s, r, len, t);
+    trav_begin<kCount>(s, r, len, id, t);   // the plane or sphere hit stays the answer unless a triangle is closer
 }
 
 template <bool kCount, class Work, class Lane>
@@ -61,8 +61,6 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
     Ray r;
     FastTrav t;
     TravStack stk;
-    float len0 = kRayLengthMax;   // distance after planes and spheres
-    uint32_t id0 = MRT_HIT_NONE;
     for (;;) {
         // 1. refill idle lanes (one atomic per warp)
         const uint32_t idle = __ballot_sync(FULL, !active);
@@ -75,7 +73,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             if (!active) {
                 const uint32_t item = base + __popc(idle & ((1u << lane_id) - 1u));
                 if (item < total && work.begin(item, lane, r)) {
-                    start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t, len0, id0);
+                    start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t);
                     active = true;
                 }
             }
@@ -94,12 +92,11 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
         if (active && trav_has_leaf(t)) trav_leaf_step<kCount>(work.view(lane, s), r, t);
         // 4. completion
         if (active && trav_finished(t)) {
-            float len = len0;
-            uint32_t id = id0;
-            if (t.have) { len = t.best_t; id = hid(MRT_PRIM_TRIANGLE, t.best_i); }
+            float len = t.best_t;
+            uint32_t id = t.best_id;
             const bool hit_light = lights_trace(work.scene(lane, s), r, len, id);
             const bool hit = id != MRT_HIT_NONE || hit_light;
-            if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t, len0, id0);
+            if (work.finish(lane, r, hit, len, id, t)) start_ray<kCount, Work, Lane>(work.scene(lane, s), r, t);
             else active = false;
         }
     }
@@ -117,9 +114,9 @@ namespace mrt {
 // the any-hit query keeps the shadow distance in best_t; planes and spheres are tested in order
 // first, then the tree, where the first occluding triangle ends the query
 __device__ __forceinline__ void occ_begin(const DevScene &s, const Ray &r, float dist, FastTrav &t) {
-    trav_begin<false>(s, r, dist, t);
+    trav_begin<false>(s, r, dist, MRT_HIT_NONE, t);
     if (naive_occ<kPlane>(s, r, dist) || naive_occ<kSphere>(s, r, dist)) {
-        t.have = true;
+        trav_set_occluded(t);
         trav_clear(t);
     }
 }
@@ -162,7 +159,7 @@ __device__ void persistent_any(const DevScene &s, Work &work, Lane &lane) {
         }
         if (active && trav_has_leaf(t)) trav_occ_leaf_step(work.view(lane, s), r, t);
         if (active && trav_finished(t)) {
-            work.finish(lane, t.have);
+            work.finish(lane, trav_hit(t));
             active = false;
         }
     }

@@ -133,9 +133,11 @@ struct NsWork {
     }
 };
 
-// resident blocks of 128 threads per SM for the NoShadows kernel (registers per thread: 65536 / (128 x this))
+// resident blocks of 128 threads per SM for the NoShadows kernel (registers per thread: 65536 / (128 x this)).
+// 6 (80 registers, no spills) beats 8 (64 registers, spills reloaded in the traversal loop) by 3 %
+// and 7 by 2 % on the 1,000,000-triangle soup frame.
 #ifndef MRT_NS_BLOCKS_PER_SM
-#define MRT_NS_BLOCKS_PER_SM 8
+#define MRT_NS_BLOCKS_PER_SM 6
 #endif
 constexpr int kNsBlocksPerSm = MRT_NS_BLOCKS_PER_SM;
 
@@ -195,32 +197,32 @@ __global__ void __launch_bounds__(128) k_wave_extend(DevScene s, WaveState w, in
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
-// the level's rays sorted into the per-material shade queues: one atomic per warp and class
-// (warp ballot over the class, popc for the lane's rank)
-__global__ void __launch_bounds__(128) k_wave_classify(DevScene s, RenderParams p, WaveState w, int level) {
-    const Level L = clamp_level(w, w.levels[level]);
-    const uint32_t n_iter = (L.count + blockDim.x - 1) / blockDim.x;
-    const int lane = threadIdx.x & 31;
-    uint32_t *count = w.class_count + kShadeClasses * level;
-    for (uint32_t it_ = blockIdx.x; it_ < n_iter; it_ += gridDim.x) {
-        const uint32_t i = it_ * blockDim.x + threadIdx.x;
-        const bool active = i < L.count;
-        const uint32_t idx = L.start + (active ? i : 0u);
-        const uint32_t c = active ? shade_class(s, p, w.rays[idx], w.nodes[idx].hit_id) : 0u;
-#pragma unroll
-        for (uint32_t k = 0; k < (uint32_t)kShadeClasses; ++k) {
-            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, active && c == k);
-            if (!mask) continue;
-            const int leader = __ffs(mask) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(&count[k], (uint32_t)__popc(mask));
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            if (active && c == k) {
-                const uint32_t pos = base + __popc(mask & ((1u << lane) - 1u));
-                if (pos < w.order_cap) w.order[(size_t)k * w.order_cap + pos] = idx;
-            }
-        }
+// one ray of a level shaded; every lane of the warp calls this (the child and shadow queues are
+// allocated once per warp)
+__device__ __forceinline__ void shade_slot(const DevScene &s, const RenderParams &p, const WaveState &w, int level,
+                                           Level *next, uint32_t next_start, bool active, uint32_t idx) {
+    ShadeLane o;
+    o.n_child = 0;
+    o.child_mask = 0;
+    o.n_shadow = 0;
+    o.shaded = false;
+    RayRec rr;
+    Stream st;
+    if (active) {
+        rr = w.rays[idx];
+        Task k;
+        uint32_t pixel, sample;
+        root_task(p, w, rr.root, k, pixel, sample);
+        st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+        shade_ray(s, p, rr, w.nodes[idx].hit_id, w.nodes[idx].hit_t, st, o);
+        store_node(w.nodes[idx], o.nd);
     }
+    // queue compaction: one atomic per warp for children, one for shadow rays
+    const uint32_t cbase = warp_alloc(o.n_child, &next->count);
+    const uint32_t sbase = warp_alloc(o.n_shadow, &w.levels[level].shadow_count);
+    if (!active) return;
+    emit_children(s, o, rr, st, idx, next_start + cbase, w.rays, w.ray_cap);
+    emit_shadows(s, p, st, o, rr, idx, sbase, w.shadows, w.shadow_cap);
 }
 
 __global__ void __launch_bounds__(128) k_wave_shade(DevScene s, RenderParams p, WaveState w, int level) {
@@ -229,39 +231,78 @@ __global__ void __launch_bounds__(128) k_wave_shade(DevScene s, RenderParams p, 
     if (blockIdx.x == 0 && threadIdx.x == 0) next->start = L.start + L.count;
     const uint32_t next_start = L.start + L.count;
     const uint32_t n_iter = (L.count + blockDim.x - 1) / blockDim.x;   // whole warps iterate together
-    uint32_t qn[kShadeClasses] = {0, 0, 0};
-    if (w.order)
-        for (int k = 0; k < kShadeClasses; ++k) qn[k] = min(w.class_count[kShadeClasses * level + k], w.order_cap);
     for (uint32_t it_ = blockIdx.x; it_ < n_iter; it_ += gridDim.x) {
         const uint32_t i = it_ * blockDim.x + threadIdx.x;
         const bool active = i < L.count;
-        uint32_t idx = L.start + (active ? i : 0);
-        if (w.order && active) {   // the i-th ray of the queues in class order
-            if (i < qn[0]) idx = w.order[i];
-            else if (i < qn[0] + qn[1]) idx = w.order[(size_t)w.order_cap + (i - qn[0])];
-            else if (i < qn[0] + qn[1] + qn[2]) idx = w.order[2 * (size_t)w.order_cap + (i - qn[0] - qn[1])];
+        shade_slot(s, p, w, level, next, next_start, active, L.start + (active ? i : 0u));
+    }
+}
+
+// Per-material shade queues for scenes that mix diffuse with mirror / glass materials: a block takes
+// a window of kSortRounds x 128 consecutive rays of the level, sorts them by shading class in shared
+// memory (one warp ballot per class and round; the class sizes by shared-memory atomics of the
+// ballots' popc, then each ray's place = its class's offset + its warp's share + its rank among the
+// ballot's lanes) and shades the window in that order, so that all but at most two warps of a
+// window run one material branch.  The reordered reads stay within the window's 180 KB of ray and
+// node records, most of them in L1 or L2 (a global sort of the level scatters every record access,
+// and its extra pass cost more than the divergence it removed).
+constexpr int kSortRounds = 8;
+__global__ void __launch_bounds__(128) k_wave_shade_sorted(DevScene s, RenderParams p, WaveState w, int level) {
+    __shared__ uint32_t s_idx[kSortRounds * 128];
+    __shared__ uint32_t s_cnt[kShadeClasses], s_fill[kShadeClasses];
+    const Level L = clamp_level(w, w.levels[level]);
+    Level *next = &w.levels[level + 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) next->start = L.start + L.count;
+    const uint32_t next_start = L.start + L.count;
+    const uint32_t win = kSortRounds * 128u;
+    const uint32_t n_win = (L.count + win - 1) / win;
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    for (uint32_t wi = blockIdx.x; wi < n_win; wi += gridDim.x) {
+        const uint32_t base = wi * win;
+        const uint32_t n_here = min(win, L.count - base);
+        if (threadIdx.x < kShadeClasses) {
+            s_cnt[threadIdx.x] = 0;
+            s_fill[threadIdx.x] = 0;
         }
-        ShadeLane o;
-        o.n_child = 0;
-        o.n_shadow = 0;
-        o.shaded = false;
-        RayRec rr;
-        Stream st;
-        if (active) {
-            rr = w.rays[idx];
-            Task k;
-            uint32_t pixel, sample;
-            root_task(p, w, rr.root, k, pixel, sample);
-            st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
-            shade_ray(s, p, rr, w.nodes[idx].hit_id, w.nodes[idx].hit_t, st, o);
-            w.nodes[idx] = o.nd;
+        __syncthreads();
+        uint32_t classes = 0;   // 2 bits per round; 3 = no ray
+#pragma unroll
+        for (int r = 0; r < kSortRounds; ++r) {
+            const uint32_t j = r * 128u + threadIdx.x;
+            const uint32_t idx = L.start + base + j;
+            const uint32_t c = j < n_here ? shade_class(s, p, w.rays[idx], w.nodes[idx].hit_id) : 3u;
+            classes |= c << (2 * r);
+#pragma unroll
+            for (uint32_t k = 0; k < (uint32_t)kShadeClasses; ++k) {
+                const uint32_t m = __ballot_sync(FULL, c == k);
+                if (lane == 0 && m) atomicAdd(&s_cnt[k], (uint32_t)__popc(m));
+            }
         }
-        // queue compaction: one atomic per warp for children, one for shadow rays
-        const uint32_t cbase = warp_alloc(o.n_child, &next->count);
-        const uint32_t sbase = warp_alloc(o.n_shadow, &w.levels[level].shadow_count);
-        if (!active) continue;
-        emit_children(s, o, rr, idx, next_start + cbase, w.rays, w.ray_cap);
-        emit_shadows(s, p, st, o, rr, idx, sbase, w.shadows, w.shadow_cap);
+        __syncthreads();
+        const uint32_t off[kShadeClasses] = {0u, s_cnt[0], s_cnt[0] + s_cnt[1]};
+#pragma unroll
+        for (int r = 0; r < kSortRounds; ++r) {
+            const uint32_t c = (classes >> (2 * r)) & 3u;
+#pragma unroll
+            for (uint32_t k = 0; k < (uint32_t)kShadeClasses; ++k) {
+                const uint32_t m = __ballot_sync(FULL, c == k);
+                if (!m) continue;
+                const int leader = __ffs(m) - 1;
+                uint32_t b = 0;
+                if (lane == leader) b = atomicAdd(&s_fill[k], (uint32_t)__popc(m));
+                b = __shfl_sync(FULL, b, leader);
+                if (c == k) s_idx[off[k] + b + __popc(m & lanes_below)] = base + r * 128u + threadIdx.x;
+            }
+        }
+        __syncthreads();
+        for (int r = 0; r < kSortRounds; ++r) {
+            const uint32_t j = r * 128u + threadIdx.x;
+            const bool active = j < n_here;
+            shade_slot(s, p, w, level, next, next_start, active, L.start + (active ? s_idx[j] : 0u));
+        }
+        __syncthreads();   // s_idx and the counts are reused by the next window
     }
 }
 
@@ -402,15 +443,21 @@ __global__ void __launch_bounds__(128) k_wave_resolve(DevScene s, RenderParams p
     const Level L = clamp_level(w, w.levels[level]);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
         const uint32_t idx = L.start + i;
-        const NodeRec nd = w.nodes[idx];
-        const RayRec rr = w.rays[idx];
-        Task k;
-        uint32_t pixel, sample;
-        root_task(p, w, rr.root, k, pixel, sample);
-        const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
-        V3 rgb;
-        bool flag;
-        resolve_node(s, p, nd, rr, st, rgb, flag);
+        const NodeRec &nd = w.nodes[idx];
+        const RayRec &rr = w.rays[idx];
+        V3 rgb{0.0f, 0.0f, 0.0f};
+        bool flag = false;
+        const uint32_t kind = nd.flags & 3u;
+        if (kind == kEmit) {
+            rgb = nd.point;
+            flag = true;
+        } else if (kind == kShaded) {   // misses and cut nodes are black
+            Task k;
+            uint32_t pixel, sample;
+            root_task(p, w, rr.root, k, pixel, sample);
+            const Stream st = make_stream(p.seed, pixel, sample, p.strata, p.constant_value);
+            resolve_node(s, p, nd, rr, st, rgb, flag);
+        }
         if (rr.parent == 0xFFFFFFFFu) {
             w.root_rgb[rr.root] = make_float4(rgb.x, rgb.y, rgb.z, flag ? 1.0f : 0.0f);
         } else {
@@ -538,15 +585,15 @@ void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState
     if (ACCEL == MRT_ACCEL_BVH && MODE == MRT_BVH_FAST) {
         // counters [2 * level] and [2 * level + 1] were zeroed for this wave
         k_wave_extend_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
-        if (w.order) k_wave_classify<<<grid, 128, 0, q>>>(s, p, w, level);
-        k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
+        if (w.sort_shading) k_wave_shade_sorted<<<grid, 128, 0, q>>>(s, p, w, level);
+        else k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
         k_wave_shadow_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level + 1);
         return;
     }
     if (ACCEL == MRT_ACCEL_REGULAR_GRID) k_wave_extend_grid<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
     else k_wave_extend<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
-    if (w.order) k_wave_classify<<<grid, 128, 0, q>>>(s, p, w, level);
-    k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
+    if (w.sort_shading) k_wave_shade_sorted<<<grid, 128, 0, q>>>(s, p, w, level);
+    else k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
     k_wave_shadow<ACCEL, MODE><<<grid, 128, 0, q>>>(s, w, level);
 }
 
@@ -696,10 +743,6 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[4], sizeof(Level) * (levels + 2));
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[5], sizeof(float4) * wave);
         if (st == MRT_OK) st = ensure(ctx, ctx->wave[6], 16);
-        // per-material shade queues where the scene mixes diffuse with mirror / glass materials
-        const bool queues = kShadeQueues && !paths && s->mixed_materials;
-        if (queues && st == MRT_OK)
-            st = ensure(ctx, ctx->wave[0], 4ull * kShadeClasses * (ray_cap + (uint64_t)levels + 1));
         if (st != MRT_OK) return st;
         WaveState w{};
         w.rays = (RayRec *)ctx->wave[1].ptr;
@@ -710,11 +753,8 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         w.counters = (unsigned long long *)ctx->wave[6].ptr;
         w.ray_cap = (uint32_t)ray_cap;
         w.shadow_cap = (uint32_t)shadow_cap;
-        if (queues) {
-            w.order = (uint32_t *)ctx->wave[0].ptr;
-            w.order_cap = (uint32_t)ray_cap;
-            w.class_count = w.order + (size_t)kShadeClasses * ray_cap;
-        }
+        // per-material shade queues where the scene mixes diffuse with mirror / glass materials
+        w.sort_shading = kShadeQueues && s->mixed_materials;
         cudaMemsetAsync(w.counters, 0, 16, q);
         // at most one wave queued ahead of the one running: a stop request ends the render within two
         // waves, and progress counts finished waves
@@ -739,7 +779,6 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 } else {
                     cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
                     cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
-                    if (w.class_count) cudaMemsetAsync(w.class_count, 0, 4ull * kShadeClasses * (levels + 1), q);
                     k_wave_raygen<<<grid, 128, 0, q>>>(p, w);
                     for (int b = 0; b < levels; ++b)
                         MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);

@@ -411,6 +411,27 @@ __device__ __forceinline__ float grid_offset(uint32_t w, uint32_t sel) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, sel));
 }
 
+// three-input minimum and maximum (one instruction each on sm_100; NaN inputs are ignored as by
+// fminf / fmaxf)
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// bit s of an 8-bit slot mask moved to bit s ^ oct (the visiting key of slot s)
+__device__ __forceinline__ uint32_t slots_to_keys(uint32_t m, uint32_t oct) {
+    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu);
+    return m;
+}
+
 template <class S>
 __device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const FastRay &f, const V3 &o, float tmax) {
     const uint4 *p = reinterpret_cast<const uint4 *>(s.fnodes) + (size_t)node * (kNodeWords / 4);
@@ -430,11 +451,10 @@ __device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const F
     const uint32_t ny = 0x7410u + ((f.oct & 2u) ? 0x22u : 0u);
     const uint32_t nz = 0x7410u + ((f.oct & 4u) ? 0x22u : 0u);
     const uint32_t imask = h0.w >> 24;
-    uint32_t groups = 0, tris = 0;
+    uint32_t hits = 0;   // slot k's box may be touched: bit k
 #pragma unroll
     for (int half = 0; half < 2; ++half) {   // four children at a time: fewer registers live
         const uint4 xq = __ldg(p + 2 + half), yq = __ldg(p + 4 + half), zq = __ldg(p + 6 + half);
-        const uint32_t meta4 = half ? h1.w : h1.z;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int k = 4 * half + j;
@@ -442,16 +462,18 @@ __device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const F
             const float tnx = __fmaf_rd(grid_offset(wx, nx), ax, lox), tfx = __fmaf_ru(grid_offset(wx, nx ^ 0x22u), ax, hix);
             const float tny = __fmaf_rd(grid_offset(wy, ny), ay, loy), tfy = __fmaf_ru(grid_offset(wy, ny ^ 0x22u), ay, hiy);
             const float tnz = __fmaf_rd(grid_offset(wz, nz), az, loz), tfz = __fmaf_ru(grid_offset(wz, nz ^ 0x22u), az, hiz);
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-            if (tn <= tf * 1.000001f) {
-                const uint32_t meta = (meta4 >> (8 * j)) & 0xFFu;
-                tris |= (meta >> 5) << (meta & 31u);
-                groups |= ((imask >> k) & 1u) << (k ^ f.oct);
-            }
+            const float tn = max3f(tnx, tny, fmaxf(tnz, 0.0f));
+            const float tf = min3f(tfx, tfy, fminf(tfz, tmax));
+            if (tn <= tf * 1.000001f) hits |= 1u << k;
         }
     }
-    return NodeHits{h1.x, (imask << 8) | groups, h1.y, tris};
+    // the triangles of the leaf children hit (meta byte k: triangle bits << 5 | offset)
+    uint32_t tris = 0;
+    for (uint32_t lh = hits & ~imask; lh; lh &= lh - 1u) {
+        const uint32_t meta = __byte_perm(h1.z, h1.w, (uint32_t)(__ffs(lh) - 1)) & 0xFFu;
+        tris |= (meta >> 5) << (meta & 31u);
+    }
+    return NodeHits{h1.x, (imask << 8) | slots_to_keys(hits & imask, f.oct), h1.y, tris};
 }
 
 // node index of the child at visiting key `key` of a group (child base, imask << 8 | ...)
@@ -462,7 +484,7 @@ __device__ __forceinline__ uint32_t group_node(uint32_t base, uint32_t groups, u
 
 template <bool kCount, class S>
 __device__ __forceinline__ void fast_tris(const S &s, const Ray &r, uint32_t base, uint32_t bits, float &best_t,
-                                          uint32_t &best_i, bool &have, FastCounts &cnt) {
+                                          uint32_t &best_id, FastCounts &cnt) {
     while (bits) {
         const uint32_t k = base + (uint32_t)(__ffs(bits) - 1);
         bits &= bits - 1u;
@@ -471,14 +493,15 @@ __device__ __forceinline__ void fast_tris(const S &s, const Ray &r, uint32_t bas
         const float4 AB = __ldg(&s.ftris[3 * (size_t)k + 1]);
         const float4 AC = __ldg(&s.ftris[3 * (size_t)k + 2]);
         if (kCount) cnt.tris++;
-        const uint32_t idx = __float_as_uint(A.w);
-        if (r.exclude == hid(MRT_PRIM_TRIANGLE, idx)) continue;
+        const uint32_t id = hid(MRT_PRIM_TRIANGLE, __float_as_uint(A.w));
+        if (r.exclude == id) continue;
         float t, u, v;
         if (!tri_test(v3(A), v3(AB), v3(AC), r, t, u, v)) continue;
-        if (t < best_t || (t == best_t && idx < best_i)) {
+        // a tie goes to the lower triangle index; a plane or sphere found first (smaller ids) and
+        // the incoming length with no hit (MRT_HIT_NONE) keep a tie, as the reference's strict `<`
+        if (t < best_t || (t == best_t && id < best_id && best_id != MRT_HIT_NONE)) {
             best_t = t;
-            best_i = idx;
-            have = true;
+            best_id = id;
         }
     }
 }
@@ -506,26 +529,29 @@ constexpr int kFastStack = 64;   // the tree is at most 62 levels deep (30-bit M
 
 struct FastTrav {
     FastRay f;
-    float best_t;
-    uint32_t best_i;
+    float best_t;      // closest hit so far (any hit: the shadow distance)
+    uint32_t best_id;  // its hit id: the plane or sphere hit before the tree, MRT_HIT_NONE, or a
+                       // triangle (for an any-hit query: a triangle id once occluded)
     uint32_t g_base, g_bits;     // node group being expanded: child base, imask << 8 | keys left
     uint32_t t_base, t_bits;     // triangles waiting for the leaf phase
     uint32_t t2_base, t2_bits;   // a second group of them, found while the warp still searched
     int sp;
-    bool have;
     uint32_t c_nodes, c_tris;
 };
+
+// the tree answered: a triangle is the closest hit (any hit: an occluder was found)
+__device__ __forceinline__ bool trav_hit(const FastTrav &t) { return MRT_HIT_TYPE(t.best_id) == MRT_PRIM_TRIANGLE; }
+__device__ __forceinline__ void trav_set_occluded(FastTrav &t) { t.best_id = hid(MRT_PRIM_TRIANGLE, 0u); }
 
 struct TravStack {
     uint2 e[kFastStack];
 };
 
 template <bool kCount, class S>
-__device__ __forceinline__ void trav_begin(const S &s, const Ray &r, float len0, FastTrav &t) {
+__device__ __forceinline__ void trav_begin(const S &s, const Ray &r, float len0, uint32_t id0, FastTrav &t) {
     t.f = fast_ray(r);
     t.best_t = len0;
-    t.best_i = 0;   // ties with a plane/sphere distance never win (index < 0 is impossible)
-    t.have = false;
+    t.best_id = id0;
     t.g_base = 0;
     // the root as the only internal child (slot 0) of a virtual group
     t.g_bits = s.n_tri == 0 ? 0u : ((1u << 8) | (1u << t.f.oct));
@@ -592,8 +618,8 @@ __device__ __forceinline__ void trav_node_step(const S &s, const Ray &r, FastTra
 template <bool kCount, class S>
 __device__ __forceinline__ void trav_leaf_step(const S &s, const Ray &r, FastTrav &t) {
     FastCounts cnt{0, 0};
-    fast_tris<kCount>(s, r, t.t_base, t.t_bits, t.best_t, t.best_i, t.have, cnt);
-    if (t.t2_bits) fast_tris<kCount>(s, r, t.t2_base, t.t2_bits, t.best_t, t.best_i, t.have, cnt);
+    fast_tris<kCount>(s, r, t.t_base, t.t_bits, t.best_t, t.best_id, cnt);
+    if (t.t2_bits) fast_tris<kCount>(s, r, t.t2_base, t.t2_bits, t.best_t, t.best_id, cnt);
     if (kCount) t.c_tris += cnt.tris;
     t.t_bits = 0;
     t.t2_bits = 0;
@@ -605,7 +631,7 @@ template <class S>
 __device__ __forceinline__ void trav_occ_leaf_step(const S &s, const Ray &r, FastTrav &t) {
     if (fast_tris_occ(s, r, t.t_base, t.t_bits, t.best_t) ||
         (t.t2_bits && fast_tris_occ(s, r, t.t2_base, t.t2_bits, t.best_t))) {
-        t.have = true;
+        trav_set_occluded(t);
         trav_clear(t);
         return;
     }
@@ -620,7 +646,7 @@ __device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t
     if (s.n_tri == 0) return false;
     FastTrav t;
     TravStack st;
-    trav_begin<kCount>(s, r, len, t);
+    trav_begin<kCount>(s, r, len, id, t);
     uint32_t steps = 0;
     while (!trav_finished(t)) {
         if (trav_has_leaf(t)) {
@@ -631,9 +657,9 @@ __device__ bool fast_trace(const DevScene &s, const Ray &r, float &len, uint32_t
         }
     }
     if (counts) *counts = FastCounts{t.c_nodes, t.c_tris};
-    if (!t.have) return false;
+    if (!trav_hit(t)) return false;
     len = t.best_t;
-    id = hid(MRT_PRIM_TRIANGLE, t.best_i);
+    id = t.best_id;
     return true;
 }
 
@@ -641,7 +667,7 @@ __device__ inline bool fast_occ(const DevScene &s, const Ray &r, float dist) {
     if (s.n_tri == 0) return false;
     FastTrav t;
     TravStack st;
-    trav_begin<false>(s, r, dist, t);
+    trav_begin<false>(s, r, dist, MRT_HIT_NONE, t);
     uint32_t steps = 0;
     while (!trav_finished(t)) {
         if (trav_has_leaf(t)) {
@@ -651,7 +677,7 @@ __device__ inline bool fast_occ(const DevScene &s, const Ray &r, float dist) {
             trav_node_step<false>(s, r, t, st);
         }
     }
-    return t.have;
+    return trav_hit(t);
 }
 
 // ---------------------------------------------------------------------------------------------

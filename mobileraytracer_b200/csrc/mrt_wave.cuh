@@ -185,13 +185,9 @@ struct WaveState {
     uint32_t root_first;     // global index of the wave's first root
     uint32_t n_roots;
     unsigned long long *counters;   // [0] closest rays, [1] shadow rays
-    // per-material shade queues (nullptr: the shade kernel takes the level's rays in order): after
-    // the closest hits of a level, its rays are sorted by shading class (kShadeClasses queues of
-    // order_cap entries, their lengths in class_count[kShadeClasses * level + c]) so that the warps
-    // of the shade kernel run one material branch each
-    uint32_t *order;
-    uint32_t *class_count;
-    uint32_t order_cap;
+    // per-material shade queues: the shade kernel sorts each window of a level's rays by shading
+    // class before shading them (scenes that mix diffuse with mirror / glass materials)
+    uint32_t sort_shading;
 };
 
 // shading class of a ray after its closest hit: 0 nothing to shade here (a miss, a ray beyond the
@@ -260,12 +256,12 @@ __device__ __forceinline__ Level clamp_level(const WaveState &w, Level L) {
 // ---------------------------------------------------------------------------------------------
 struct ShadeLane {
     NodeRec nd;
-    Ray child[3];
-    uint32_t child_slot[3];
+    uint32_t child_mask;   // continuation rays: bit 0 indirect, 1 specular, 2 transmission
     uint32_t n_child;
     uint32_t n_shadow;
     bool shaded;
-    Isect isect;
+    uint32_t prim;         // Isect::prim: excluded from the continuation and shadow rays
+    float ior;
 };
 
 // the part of Whitted::shade / PathTracer::shade before their recursive calls
@@ -286,7 +282,8 @@ __device__ __forceinline__ void shade_ray(const DevScene &s, const RenderParams 
     nd.point = nd.normal = V3{0, 0, 0};
     nd.hit_id = hit_id;
     nd.hit_t = hit_t;
-    Isect &isect = o.isect;
+    o.child_mask = 0;
+    Isect isect;
     if (hit_id == MRT_HIT_NONE || !make_isect(s, r, hit_id, isect)) return;
     if (r.depth > p.depth_max) {
         nd.flags = kCut;   // Whitted.cpp:20-22, PathTracer.cpp:28-31
@@ -324,50 +321,61 @@ __device__ __forceinline__ void shade_ray(const DevScene &s, const RenderParams 
         if (go) {
             nd.flags |= kHasIndirect;
             if (r.depth > p.depth_min) nd.flags |= kRRScaled;
-            Ray c;
-            c.o = isect.point;
-            c.d = hemisphere(isect.normal, key_float(st.base, rr.code, kDimHemi), key_float(st.base, rr.code, kDimHemi + 1u));
-            c.depth = r.depth + 1;
-            c.exclude = isect.prim;
-            o.child[o.n_child] = c;
-            o.child_slot[o.n_child++] = 0;
+            o.child_mask |= 1u;
         }
     }
-    if (ks_pos) {
-        Ray c;
-        c.o = isect.point;
-        c.d = reflect(r.d, isect.normal);
-        c.depth = r.depth + 1;
-        c.exclude = isect.prim;
-        o.child[o.n_child] = c;
-        o.child_slot[o.n_child++] = 1;
-    }
-    if (kt_pos) {
-        Ray c;
-        c.o = isect.point;
-        c.d = refract(r.d, isect.normal, 1.0f / ior);
-        c.depth = r.depth + 1;
-        c.exclude = isect.prim;
-        o.child[o.n_child] = c;
-        o.child_slot[o.n_child++] = 2;
-    }
+    if (ks_pos) o.child_mask |= 2u;
+    if (kt_pos) o.child_mask |= 4u;
+    o.n_child = __popc(o.child_mask);
+    o.prim = isect.prim;
+    o.ior = ior;
 }
 
-__device__ __forceinline__ void emit_children(const DevScene &s, const ShadeLane &o, const RayRec &rr, uint32_t idx,
-                                              uint32_t pos0, RayRec *rays, uint32_t cap) {
-    for (uint32_t c = 0; c < o.n_child; ++c) {
-        const uint32_t pos = pos0 + c;
+// the node record as the resolve pass reads it: a miss or a cut node only its flags, an emitter
+// its radiance, a shaded node its terms with the occlusion and child-flag bits cleared (the
+// children's values arrive from their own resolve)
+__device__ __forceinline__ void store_node(NodeRec &dst, const NodeRec &nd) {
+    dst.flags = nd.flags;
+    const uint32_t kind = nd.flags & 3u;
+    if (kind == kEmit) dst.point = nd.point;
+    if (kind != kShaded) return;
+    dst.occluded = 0;
+    dst.child_flag = 0;
+    dst.kd = nd.kd;
+    dst.ks = nd.ks;
+    dst.kt = nd.kt;
+    dst.point = nd.point;
+    dst.normal = nd.normal;
+}
+
+// the direction of the continuation ray of `slot` from a shaded node (the hemisphere sample of the
+// indirect ray, PathTracer.cpp:106-134; mirror and refraction, Whitted.cpp:85-104,
+// PathTracer.cpp:136-157); d = the incoming direction, code = the node's path-tree code
+__device__ __forceinline__ V3 child_dir(const ShadeLane &o, const V3 &d, const Stream &st, uint32_t code, uint32_t slot) {
+    if (slot == 0u) return hemisphere(o.nd.normal, key_float(st.base, code, kDimHemi), key_float(st.base, code, kDimHemi + 1u));
+    if (slot == 1u) return reflect(d, o.nd.normal);
+    return refract(d, o.nd.normal, 1.0f / o.ior);
+}
+
+// the continuation rays in slot order, from the hit point
+__device__ __forceinline__ void emit_children(const DevScene &s, const ShadeLane &o, const RayRec &rr, const Stream &st,
+                                              uint32_t idx, uint32_t pos0, RayRec *rays, uint32_t cap) {
+    const V3 d{rr.dx, rr.dy, rr.dz};
+    uint32_t pos = pos0;
+    for (uint32_t m = o.child_mask; m; m &= m - 1u) {
+        const uint32_t slot = (uint32_t)(__ffs(m) - 1);
         if (pos >= cap) { raise_error(s, MRT_ERR_LIMIT); break; }
+        const V3 cd = child_dir(o, d, st, rr.code, slot);
         RayRec q;
-        q.ox = o.child[c].o.x; q.oy = o.child[c].o.y; q.oz = o.child[c].o.z;
-        q.dx = o.child[c].d.x; q.dy = o.child[c].d.y; q.dz = o.child[c].d.z;
-        q.depth = o.child[c].depth;
-        q.exclude = o.child[c].exclude;
+        q.ox = o.nd.point.x; q.oy = o.nd.point.y; q.oz = o.nd.point.z;
+        q.dx = cd.x; q.dy = cd.y; q.dz = cd.z;
+        q.depth = rr.depth + 1;
+        q.exclude = o.prim;
         q.root = rr.root;
         q.parent = idx;
-        q.slot = o.child_slot[c];
-        q.code = rr.code * 4u + o.child_slot[c] + 1u;
-        rays[pos] = q;
+        q.slot = slot;
+        q.code = rr.code * 4u + slot + 1u;
+        rays[pos++] = q;
     }
 }
 
@@ -380,19 +388,19 @@ __device__ __forceinline__ void emit_shadows(const DevScene &s, const RenderPara
     for (uint32_t j = 0; j < p.spl; ++j) {
         const DevLight &l = pick_light(s, st, rr.code, j);
         const V3 lp = light_position(l, st, p.light_sampler, rr.code, j);
-        V3 vtl = lp - o.isect.point;
+        V3 vtl = lp - o.nd.point;
         const float dist = length(vtl);
         vtl = normalize(vtl);
-        if (!(dot(o.isect.normal, vtl) > 0.0f)) continue;
+        if (!(dot(o.nd.normal, vtl) > 0.0f)) continue;
         const uint32_t pos = pos0 + q++;
         if (pos >= cap) { raise_error(s, MRT_ERR_LIMIT); break; }
         ShadowRec sr;
-        sr.ox = o.isect.point.x; sr.oy = o.isect.point.y; sr.oz = o.isect.point.z;
+        sr.ox = o.nd.point.x; sr.oy = o.nd.point.y; sr.oz = o.nd.point.z;
         sr.dx = vtl.x; sr.dy = vtl.y; sr.dz = vtl.z;
         sr.dist = dist;
         sr.node = idx;
         sr.j = j;
-        sr.exclude = o.isect.prim;
+        sr.exclude = o.prim;
         shadows[pos] = sr;
     }
 }
