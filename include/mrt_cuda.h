@@ -187,6 +187,13 @@ typedef struct MrtCamera {
     float fov_v_deg;      /* Orthographic(position, lookAt, up, sizeH, sizeV): film size    */
 } MrtCamera;
 
+/* MrtRenderOpts.flags */
+/* Whitted / PathTracer wavefront of a scene that mixes diffuse with mirror or glass materials: sort
+ * each window of a level's rays by material class before shading them, so that a warp runs one
+ * material branch.  Off by default: on a 1024x1024 glass room (16 spp) the sorted shading was 8 %
+ * slower than shading the rays in queue order. */
+#define MRT_RENDER_SHADE_QUEUES 1u
+
 typedef struct MrtRenderOpts {
     int32_t shader;         /* MRT_SHADER_* */
     uint32_t width;         /* Renderer width_ / height_ */
@@ -202,7 +209,7 @@ typedef struct MrtRenderOpts {
     uint64_t seed;          /* stream key */
     uint32_t spp_offset;    /* index of the first sample: a progressive render continues the stream
                                and the running mean from here */
-    uint32_t reserved;
+    uint32_t flags;         /* MRT_RENDER_* bits (0: the defaults) */
     float depth_point[3];   /* DepthMap maxPoint (DepthMap.cpp:14-17): depth = max(1 - t / (2 |p - o|), 0) */
     uint32_t reserved2;
 } MrtRenderOpts;

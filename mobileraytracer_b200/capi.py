@@ -25,6 +25,7 @@ MRT_HIT_NONE = 0xFFFFFFFF
 MRT_MEM_HOST, MRT_MEM_DEVICE = 0, 1
 MRT_BATCH_SMALLEST_FIRST, MRT_BATCH_FIFO, MRT_BATCH_EQUAL_SHARE = 0, 1, 2
 MRT_BATCH_KERNEL_WAVEFRONT, MRT_BATCH_KERNEL_PATHS = 1, 2
+MRT_RENDER_SHADE_QUEUES = 1
 RAY_LENGTH_MAX = 1.0e30
 
 STATUS_NAMES = {0: "MRT_OK", 1: "MRT_ERR_ARG", 2: "MRT_ERR_OOM", 3: "MRT_ERR_CUDA", 4: "MRT_ERR_LIMIT",
@@ -91,7 +92,7 @@ class MrtRenderOpts(ctypes.Structure):
         ("spp", ctypes.c_uint32), ("spl", ctypes.c_uint32), ("pixel_sampler", ctypes.c_int32),
         ("constant_value", ctypes.c_float), ("light_sampler", ctypes.c_int32), ("rr_sampler", ctypes.c_int32),
         ("depth_min", ctypes.c_int32), ("depth_max", ctypes.c_int32), ("seed", ctypes.c_uint64),
-        ("spp_offset", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("depth_point", ctypes.c_float * 3),
+        ("spp_offset", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("depth_point", ctypes.c_float * 3),
         ("reserved2", ctypes.c_uint32),
     ]
 
@@ -138,7 +139,7 @@ class MrtServeStats(ctypes.Structure):
 
 def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1, pixel_sampler=None,
                 constant_value=0.5, light_sampler=MRT_SAMPLER_RANDOM, rr_sampler=MRT_SAMPLER_RANDOM,
-                depth_min=4, depth_max=8, seed=0, spp_offset=0, depth_point=(1.0, 1.0, 1.0)) -> MrtRenderOpts:
+                depth_min=4, depth_max=8, seed=0, spp_offset=0, depth_point=(1.0, 1.0, 1.0), flags=0) -> MrtRenderOpts:
     """Options with the reference CLI's wiring as defaults (c_wrapper.cpp:436-443,455): the pixel
     sampler is Constant(0.5) at 1 spp and random otherwise; RayDepthMin 4, RayDepthMax 8."""
     if pixel_sampler is None:
@@ -149,6 +150,7 @@ def render_opts(shader=MRT_SHADER_NOSHADOWS, width=256, height=256, spp=1, spl=1
     o.light_sampler, o.rr_sampler = light_sampler, rr_sampler
     o.depth_min, o.depth_max, o.seed, o.spp_offset = depth_min, depth_max, seed, spp_offset
     o.depth_point[:] = depth_point
+    o.flags = flags
     return o
 
 

@@ -23,7 +23,10 @@ namespace mrt {
 // the node phase of a warp ends when no lane searches any more, or when fewer than kNodeQuorum lanes
 // search while others hold leaves: those leaves are tested first, and the few searching lanes go on
 // in the next node phase (2 and 4: +2 % on the 1,000,000-triangle soup frame, 8: -2 %)
-constexpr int kNodeQuorum = 4;
+#ifndef MRT_NODE_QUORUM
+#define MRT_NODE_QUORUM 4
+#endif
+constexpr int kNodeQuorum = MRT_NODE_QUORUM;
 __device__ __forceinline__ bool node_phase_over(bool searching, bool holding_leaf) {
     const uint32_t s = __ballot_sync(0xFFFFFFFFu, searching);
     return s == 0u || (__popc(s) < kNodeQuorum && __any_sync(0xFFFFFFFFu, holding_leaf));
@@ -51,8 +54,8 @@ __device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastT
     trav_begin<kCount>(s, r, len, id, t);   // the plane or sphere hit stays the answer unless a triangle is closer
 }
 
-template <bool kCount, class Work, class Lane>
-__device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
+template <bool kCount, class Work, class Lane, class Stack>
+__device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, Stack &stk) {
     const uint32_t FULL = 0xFFFFFFFFu;
     const int lane_id = threadIdx.x & 31;
     const uint32_t total = work.total();
@@ -60,7 +63,6 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
     bool exhausted = false;
     Ray r;
     FastTrav t;
-    TravStack stk;
     for (;;) {
         // 1. refill idle lanes (one atomic per warp)
         const uint32_t idle = __ballot_sync(FULL, !active);
@@ -100,6 +102,13 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
             else active = false;
         }
     }
+}
+
+// the same with the stack in local memory
+template <bool kCount, class Work, class Lane>
+__device__ __forceinline__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
+    TravStack stk;
+    persistent_closest<kCount>(s, work, lane, stk);
 }
 
 }  // namespace mrt

@@ -60,11 +60,6 @@ __global__ void __launch_bounds__(128) k_render_noshadows(DevScene s, RenderPara
     }
 }
 
-// per-material shade queues in the wavefront of scenes that mix materials (0 builds without them)
-#ifndef MRT_SHADE_QUEUES
-#define MRT_SHADE_QUEUES 1
-#endif
-constexpr bool kShadeQueues = MRT_SHADE_QUEUES != 0;
 
 // persistent FAST-BVH NoShadows: work item = pixel task; the lane traces the pixel's samples in
 // order.  Only the task number and the sample count stay in registers while a ray is traced: the
@@ -77,6 +72,15 @@ struct NsLane {
     uint32_t t;    // task number
     uint32_t si;   // samples done
 };
+
+// task of the round's item-th pixel: row-major from `first`, or in 2x16-pixel tiles handed out row
+// by row (tiles_x tiles per tile row)
+__device__ __forceinline__ uint32_t ns_task(const RenderParams &p, uint32_t first, uint32_t item, uint32_t tiles_x) {
+    if (!tiles_x) return first + item;
+    const uint32_t tile = item >> 5, w = item & 31u;
+    const uint32_t x = (tile % tiles_x) * 2u + (w & 1u), y = (tile / tiles_x) * 16u + (w >> 1);
+    return y * p.width + x;
+}
 
 struct NsWork {
     const DevScene *s;
@@ -96,13 +100,7 @@ struct NsWork {
         return primary_ray(*p, k, st);
     }
     __device__ bool begin(uint32_t item, NsLane &lane, Ray &r) const {
-        uint32_t t = first + item;
-        if (tiles_x) {
-            const uint32_t tile = item >> 5, w = item & 31u;
-            const uint32_t x = (tile % tiles_x) * 2u + (w & 1u), y = (tile / tiles_x) * 16u + (w >> 1);
-            t = y * p->width + x;
-        }
-        lane.t = t;
+        lane.t = ns_task(*p, first, item, tiles_x);
         lane.si = 0;
         r = ray_for(lane);
         return true;
@@ -133,19 +131,32 @@ struct NsWork {
     }
 };
 
-// resident blocks of 128 threads per SM for the NoShadows kernel (registers per thread: 65536 / (128 x this)).
-// 6 (80 registers, no spills) beats 8 (64 registers, spills reloaded in the traversal loop) by 3 %
-// and 7 by 2 % on the 1,000,000-triangle soup frame.
+// resident blocks of 128 threads per SM for the NoShadows traversal (registers per thread: 65536 / (128 x
+// this)).  On the 1,000,000-triangle soup frame the split trace kernel fits 72 registers without spills:
+// 7 blocks give 1507 Mrays/s against 1454 at 6 (80 registers) and 1353 at 8 (64 registers, spills).
 #ifndef MRT_NS_BLOCKS_PER_SM
-#define MRT_NS_BLOCKS_PER_SM 6
+#define MRT_NS_BLOCKS_PER_SM 7
 #endif
 constexpr int kNsBlocksPerSm = MRT_NS_BLOCKS_PER_SM;
+
+// traversal stack entries per thread kept in shared memory (0: all in local memory)
+#ifndef MRT_NS_SMEM_STACK
+#define MRT_NS_SMEM_STACK 0
+#endif
+constexpr int kNsSmemStack = MRT_NS_SMEM_STACK;
 
 __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_render_noshadows_fast(DevScene s, RenderParams p, uint32_t first,
                                                                uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
-    persistent_closest<false>(s, w, lane);
+    if constexpr (kNsSmemStack > 0) {
+        __shared__ uint2 stack_cols[(kNsSmemStack > 0 ? kNsSmemStack : 1) * 128];
+        SharedTravStack<(kNsSmemStack > 0 ? kNsSmemStack : 1), 128> stk;
+        stk.col = stack_cols + threadIdx.x;
+        persistent_closest<false>(s, w, lane, stk);
+    } else {
+        persistent_closest<false>(s, w, lane);
+    }
 }
 
 // the same work on the RegularGrid: the persistent grid walk (mrt_gridwalk.cuh), one cell per lane
@@ -155,6 +166,86 @@ __global__ void __launch_bounds__(128, 8) k_render_noshadows_grid(DevScene s, Re
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
     persistent_grid_closest(s, w, lane);
+}
+
+// NoShadows on the FAST tree in two passes over a chunk of (sample, pixel) items: the persistent
+// traversal writes each camera ray's closest hit (distance bits, hit id) to a buffer, then one
+// thread per pixel shades the chunk's samples in sample order and updates the running mean.  The
+// traversal lanes then carry nothing but their item (no shading code between node steps: fewer
+// registers, and the shading runs with every lane of a warp busy instead of the few lanes that
+// finish a ray in the same iteration).
+struct NsTraceLane {
+    uint32_t i;   // item of the chunk
+};
+
+struct NsTraceWork {
+    const RenderParams *p;
+    uint32_t first, j0, n_pix, s0, n_items, tiles_x;
+    uint32_t *ctr;
+    uint2 *hits;
+    __device__ uint32_t total() const { return n_items; }
+    __device__ uint32_t *counter() const { return ctr; }
+    template <class L>
+    __device__ const DevScene &scene(const L &, const DevScene &s) const { return s; }
+    template <class L>
+    __device__ const DevScene &view(const L &, const DevScene &s) const { return s; }
+    __device__ bool begin(uint32_t item, NsTraceLane &lane, Ray &r) const {
+        lane.i = item;
+        const uint32_t si = item / n_pix, j = item - si * n_pix;
+        const Task k = task_of(*p, ns_task(*p, first, j0 + j, tiles_x));
+        const Stream st = make_stream(p->seed, k.y * p->width + k.x, p->spp_offset + s0 + si, p->strata, p->constant_value);
+        r = primary_ray(*p, k, st);
+        return true;
+    }
+    __device__ bool finish(NsTraceLane &lane, Ray &, bool hit, float t, uint32_t id, const FastTrav &) const {
+        hits[lane.i] = make_uint2(__float_as_uint(t), hit ? id : MRT_HIT_NONE);
+        return false;
+    }
+};
+
+// the split form (0: one fused kernel traces and shades) and its chunk of items (hit buffer of 8 B each)
+#ifndef MRT_NS_SPLIT
+#define MRT_NS_SPLIT 1
+#endif
+constexpr bool kNsSplit = MRT_NS_SPLIT != 0;
+constexpr uint32_t kNsChunk = 1u << 22;
+
+__global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, NsTraceWork w, RenderParams p) {
+    w.p = &p;
+    NsTraceLane lane;
+    if constexpr (kNsSmemStack > 0) {
+        __shared__ uint2 stack_cols[(kNsSmemStack > 0 ? kNsSmemStack : 1) * 128];
+        SharedTravStack<(kNsSmemStack > 0 ? kNsSmemStack : 1), 128> stk;
+        stk.col = stack_cols + threadIdx.x;
+        persistent_closest<false>(s, w, lane, stk);
+    } else {
+        persistent_closest<false>(s, w, lane);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_ns_shade(DevScene s, RenderParams p, uint32_t first, uint32_t j0, uint32_t n_pix,
+                                                  uint32_t s0, uint32_t n_s, uint32_t tiles_x, const uint2 *__restrict__ hits) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_pix; j += gridDim.x * blockDim.x) {
+        const Task k = task_of(p, ns_task(p, first, j0 + j, tiles_x));
+        uint32_t bm = p.bitmap[k.index];
+        const int64_t slot = p.accum ? accum_slot(p, k) : -1;
+        float4 acc = slot >= 0 ? p.accum[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t si = 0; si < n_s; ++si) {
+            const uint32_t sample = p.spp_offset + s0 + si;
+            const uint2 h = hits[(size_t)si * n_pix + j];
+            V3 rgb{0.0f, 0.0f, 0.0f};
+            if (h.y != MRT_HIT_NONE) {
+                const Stream st = make_stream(p.seed, k.y * p.width + k.x, sample, p.strata, p.constant_value);
+                const Ray r = primary_ray(p, k, st);
+                Isect it;
+                if (make_isect(s, r, h.y, it)) rgb = shade_direct(s, p, st, r, it);
+            }
+            bm = incremental_avg(rgb, bm, sample + 1u);
+            acc.x += rgb.x; acc.y += rgb.y; acc.z += rgb.z; acc.w += 1.0f;
+        }
+        p.bitmap[k.index] = bm;
+        if (slot >= 0) p.accum[slot] = acc;
+    }
 }
 
 // ============================== wavefront ====================================================
@@ -374,7 +465,13 @@ struct ShadowWork {
     }
 };
 
-__global__ void __launch_bounds__(128, 8) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+// resident blocks of 128 threads per SM for the wavefront's persistent extend and shadow kernels
+#ifndef MRT_WAVE_BLOCKS_PER_SM
+#define MRT_WAVE_BLOCKS_PER_SM 8
+#endif
+constexpr int kWaveBlocksPerSm = MRT_WAVE_BLOCKS_PER_SM;
+
+__global__ void __launch_bounds__(128, kWaveBlocksPerSm) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const Level L = clamp_level(w, w.levels[level]);
     ExtendWork work{w, L, ctr};
     WaveLane lane;
@@ -390,7 +487,7 @@ __global__ void __launch_bounds__(128, 8) k_wave_extend_grid(DevScene s, WaveSta
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
-__global__ void __launch_bounds__(128, 8) k_wave_shadow_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
+__global__ void __launch_bounds__(128, kWaveBlocksPerSm) k_wave_shadow_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const uint32_t n = min(w.levels[level].shadow_count, w.shadow_cap);
     ShadowWork work{w, n, ctr};
     WaveLane lane;
@@ -706,7 +803,27 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         const uint32_t tiles_x = (plan.implicit && o->width % 2u == 0 && rows % 16u == 0) ? o->width / 2u : 0u;
         for (size_t r = 0; r < plan.round_first.size(); ++r) {
             if (s->stop.load()) return cancelled(ctx, q);
-            if (fast) {
+            if (fast && kNsSplit) {
+                // chunks of at most kNsChunk (sample, pixel) items: whole samples of up to kNsChunk pixels
+                const uint32_t count = plan.round_count[r];
+                const uint32_t n_pix_max = std::min<uint32_t>(count, kNsChunk);
+                st = ensure(ctx, ctx->wave[1], sizeof(uint2) * (size_t)kNsChunk);
+                if (st != MRT_OK) return st;
+                uint2 *hits = (uint2 *)ctx->wave[1].ptr;
+                for (uint32_t j0 = 0; j0 < count; j0 += n_pix_max) {
+                    const uint32_t n_pix = std::min(n_pix_max, count - j0);
+                    const uint32_t per = std::max(1u, kNsChunk / n_pix);
+                    for (uint32_t s0 = 0; s0 < o->spp; s0 += per) {
+                        if (s->stop.load()) return cancelled(ctx, q);
+                        const uint32_t n_s = std::min(per, o->spp - s0);
+                        NsTraceWork tw{nullptr, plan.round_first[r], j0, n_pix, s0, n_pix * n_s, tiles_x, ctx->d_counters, hits};
+                        cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
+                        k_ns_trace<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, tw, p);
+                        k_ns_shade<<<(n_pix + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0, n_pix, s0, n_s,
+                                                                        tiles_x, hits);
+                    }
+                }
+            } else if (fast) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_fast<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
@@ -754,7 +871,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         w.ray_cap = (uint32_t)ray_cap;
         w.shadow_cap = (uint32_t)shadow_cap;
         // per-material shade queues where the scene mixes diffuse with mirror / glass materials
-        w.sort_shading = kShadeQueues && s->mixed_materials;
+        w.sort_shading = (o->flags & MRT_RENDER_SHADE_QUEUES) && s->mixed_materials ? 1u : 0u;
         cudaMemsetAsync(w.counters, 0, 16, q);
         // at most one wave queued ahead of the one running: a stop request ends the render within two
         // waves, and progress counts finished waves

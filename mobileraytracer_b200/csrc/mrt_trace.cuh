@@ -543,8 +543,26 @@ struct FastTrav {
 __device__ __forceinline__ bool trav_hit(const FastTrav &t) { return MRT_HIT_TYPE(t.best_id) == MRT_PRIM_TRIANGLE; }
 __device__ __forceinline__ void trav_set_occluded(FastTrav &t) { t.best_id = hid(MRT_PRIM_TRIANGLE, 0u); }
 
+// the stack of node groups in local memory
 struct TravStack {
     uint2 e[kFastStack];
+    __device__ __forceinline__ void put(int i, uint2 v) { e[i] = v; }
+    __device__ __forceinline__ uint2 get(int i) const { return e[i]; }
+};
+
+// the first K entries in this thread's column of a block-wide shared array (entry i at col[i * B],
+// B = threads per block), the rest in local memory.  Lanes whose stacks have different depths still
+// touch distinct banks (a column per thread), where their local-memory entries would fall into
+// distinct sectors.
+template <int K, int B>
+struct SharedTravStack {
+    uint2 *col;
+    uint2 e[kFastStack - K];
+    __device__ __forceinline__ void put(int i, uint2 v) {
+        if (i < K) col[i * B] = v;
+        else e[i - K] = v;
+    }
+    __device__ __forceinline__ uint2 get(int i) const { return i < K ? col[i * B] : e[i - K]; }
 };
 
 template <bool kCount, class S>
@@ -589,11 +607,11 @@ __device__ __forceinline__ bool node_in_range(const S &s, uint32_t node) {
 
 // one node step: the next child of the current group (a group popped first when it is empty), its
 // node tested, its hit internal children becoming the current group (the rest of the old one pushed)
-template <bool kCount, class S>
-__device__ __forceinline__ void trav_node_step(const S &s, const Ray &r, FastTrav &t, TravStack &st) {
+template <bool kCount, class S, class Stack>
+__device__ __forceinline__ void trav_node_step(const S &s, const Ray &r, FastTrav &t, Stack &st) {
     if ((t.g_bits & 0xFFu) == 0u) {
         if (t.sp == 0) return;
-        const uint2 e = st.e[--t.sp];
+        const uint2 e = st.get(--t.sp);
         t.g_base = e.x;
         t.g_bits = e.y;
     }
@@ -602,7 +620,7 @@ __device__ __forceinline__ void trav_node_step(const S &s, const Ray &r, FastTra
     const uint32_t node = group_node(t.g_base, t.g_bits, key, t.f.oct);
     if (t.g_bits & 0xFFu) {
         if (t.sp >= kFastStack) { raise_error(s, MRT_ERR_LIMIT); trav_clear(t); return; }
-        st.e[t.sp++] = make_uint2(t.g_base, t.g_bits);
+        st.put(t.sp++, make_uint2(t.g_base, t.g_bits));
     }
     if (!node_in_range(s, node)) { raise_error(s, MRT_ERR_LIMIT); trav_clear(t); return; }
     const NodeHits h = node_hits(s, node, t.f, r.o, t.best_t);

@@ -69,3 +69,9 @@ def test_hit_id_encoding():
     assert capi.hit_id(capi.MRT_PRIM_TRIANGLE, 5) == (2 << 30) | 5
     assert capi.hit_id(capi.MRT_PRIM_PLANE, 0) == 0
     assert capi.MRT_HIT_NONE >> 30 == 3
+
+
+def test_render_flag_constants_match_the_header():
+    src = open(HEADER).read()
+    m = re.search(r"#define MRT_RENDER_SHADE_QUEUES (\d+)u", src)
+    assert m and int(m.group(1)) == capi.MRT_RENDER_SHADE_QUEUES

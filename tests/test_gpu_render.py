@@ -266,10 +266,12 @@ def test_whole_paths_equal_wavefront(ctx, tmp_path):
 @pytest.mark.parametrize("shader", [WH, PT])
 def test_glass_room_wavefront_with_material_queues(ctx, shader):
     """A frame above the whole-path limit (768x768 = 589,824 camera paths) of a scene that mixes
-    diffuse walls with mirror and glass spheres: the FAST-BVH wavefront sorts every level's rays into
-    per-material shade queues.  The result equals the oracle bit for bit."""
+    diffuse walls with mirror and glass spheres, rendered with MRT_RENDER_SHADE_QUEUES: the FAST-BVH
+    wavefront sorts every window of a level's rays by material class before shading.  The result
+    equals the oracle bit for bit."""
     sc = scenes.glass_room()
-    opts = capi.render_opts(shader=shader, width=768, height=768, spp=1, spl=1, seed=4)
+    opts = capi.render_opts(shader=shader, width=768, height=768, spp=1, spl=1, seed=4,
+                            flags=capi.MRT_RENDER_SHADE_QUEUES)
     bm_g, acc_g, stats, bm_o, acc_o, counts = render_both(ctx, sc, sc.camera, opts, capi.MRT_ACCEL_BVH,
                                                           capi.MRT_BVH_FAST, 3)
     assert_same(bm_g, acc_g, bm_o, acc_o, 1e-3 if shader == PT else 1e-4)
