@@ -41,7 +41,7 @@ METRIC = "Mrays/s @1 B200, batched+served vs plain GPU vs host CPU; p50/p99 job 
 FRAME = "NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point light, the CLI camera"
 WORKLOAD = FRAME + ", FAST BVH built on the device"
 REF_WORKLOAD = FRAME + ", the reference's BVH (BVH<Triangle>, top-down SAH) built on the host"
-PROFILE = os.path.join(ROOT, "profiles", "render_noshadows_soup_1080p.md")
+PROFILE = os.path.join(ROOT, "profiles", "ns_trace_soup_1080p.md")
 FAST_NODE_BYTES = 128  # bytes of one 8-wide node, the unit of the FAST tree's counting replay
 
 
@@ -335,7 +335,9 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------
 def time_frames(dist, ctx, scene, sc, opts, steps: int, warmup: int, accum: bool = False):
     """Device time of `steps` renders on device buffers, L2 flushed (512 MiB write outside the timed
-    events) before every frame; clocks sampled during the timed frames."""
+    events) before every frame; clocks sampled during the timed frames.  Returns the summed frame
+    time, rays, paths, the clock record, the summed time of the traversal launches and the count of
+    the library's kernel launches (MrtRenderStats.kernel_launches)."""
     import torch
     w, h = opts.width, opts.height
     bitmap = torch.zeros(w * h, dtype=torch.int32, device=dist.device)
@@ -354,16 +356,18 @@ def time_frames(dist, ctx, scene, sc, opts, steps: int, warmup: int, accum: bool
     dist.barrier()
     torch.cuda.synchronize()
     clocks.mark()
-    dev_ms, rays, paths = 0.0, 0, 0
+    dev_ms, trace_ms, rays, paths, launches = 0.0, 0.0, 0, 0, 0
     for _ in range(steps):
         st = step()
         dev_ms += st.device_ms
+        trace_ms += st.trace_ms
+        launches += st.kernel_launches
         rays += st.rays_closest + st.rays_shadow
         paths += st.paths
     torch.cuda.synchronize()
     clk = clocks.summary()
     del flush
-    return dev_ms, rays, paths, clk
+    return dev_ms, rays, paths, clk, trace_ms, launches
 
 
 def time_e2e(scene, sc, opts, n: int, accum: bool = False):
@@ -396,8 +400,9 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
     build_s = time.time() - t0
     info = scene.accel_info()
     opts = capi.render_opts(shader=capi.MRT_SHADER_NOSHADOWS, width=WIDTH, height=HEIGHT, spp=1, spl=1)
-    dev_ms, rays, _, clk = time_frames(dist, ctx, scene, sc, opts, args.steps, args.warmup)
+    dev_ms, rays, _, clk, trace_ms, launches = time_frames(dist, ctx, scene, sc, opts, args.steps, args.warmup)
     dev_ms = dist.max(dev_ms)
+    trace_ms = dist.max(trace_ms) / args.steps   # the traversal launch of each frame (FAST BVH)
     rays_per_step = rays // args.steps
     value = rays_per_step * args.steps * dist.ws / (dev_ms / 1e3) / 1e6
     ms = dev_ms / args.steps
@@ -415,12 +420,17 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
         counts = {"cells_per_ray": n_nodes / len(rays_np), "refs_per_ray": n_tris / len(rays_np)}
         kernel = "k_render_noshadows_grid (persistent grid walk)"
     else:
-        # result 8 + node bytes + 48 per triangle record + shading 76
-        alg = 8 * len(rays_np) + FAST_NODE_BYTES * n_nodes + 48 * n_tris + 76 * n_hit
+        # the traversal kernel: node bytes + 48 per triangle record + the 8-byte hit record written
+        alg = FAST_NODE_BYTES * n_nodes + 48 * n_tris + 8 * len(rays_np)
         counts = {"node_fetches_per_ray": n_nodes / len(rays_np), "node_fetch_bytes": FAST_NODE_BYTES,
-                  "tri_records_per_ray": n_tris / len(rays_np)}
-        kernel = "k_render_noshadows_fast (persistent)"
-    achieved = alg / (ms / 1e3) / 1e9
+                  "tri_records_per_ray": n_tris / len(rays_np), "kernel_ms": trace_ms, "frame_ms": ms,
+                  "shade_kernel": {"name": "k_ns_shade (per pixel: hit record 8 + triangle record 48 + shading 76 "
+                                           "per hit + bitmap 8)",
+                                   "algorithmic_bytes_per_launch": 16 * len(rays_np) + (48 + 76) * n_hit,
+                                   "ms": ms - trace_ms}}
+        kernel = "k_ns_trace (persistent traversal; k_ns_shade shades the frame's samples after it)"
+    kernel_ms = trace_ms if (accel != capi.MRT_ACCEL_REGULAR_GRID and trace_ms > 0) else ms
+    achieved = alg / (kernel_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
             "bytes_per_ray": alg / len(rays_np), **counts, "kernel": kernel}
@@ -431,7 +441,7 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
             scale = len(rays_np) / float(prof.get("rays_per_launch", len(rays_np)))
             traffic = float(prof["dram_bytes_per_launch"]) * scale
             roof["traffic"] = traffic
-            roof["dram_frac"] = traffic / (ms / 1e3) / 1e9 / peak
+            roof["dram_frac"] = traffic / (kernel_ms / 1e3) / 1e9 / peak
             for k in ("l1_hit_pct", "l2_hit_pct", "l1_throughput_pct", "l2_throughput_pct", "dram_throughput_pct",
                       "warps_active_pct", "lanes_active_per_inst", "issue_active_pct"):
                 if k in prof:
@@ -448,7 +458,7 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
            "build_seconds": build_s, "accel_info": info,
            "e2e": {"value": rays_per_step * dist.ws / e2e_s / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-           "gpu_launches": args.steps, "roofline": roof, "clocks": clk, "cpu_baseline": cpu}
+           "gpu_launches": launches, "roofline": roof, "clocks": clk, "cpu_baseline": cpu}
     scene.close()
     return rec
 
@@ -484,7 +494,7 @@ def scene_frame(dist, ctx, name: str, steps: int, warmup: int, args):
     t0 = time.time()
     scene = m.Scene(ctx, sc).build(capi.MRT_ACCEL_BVH, capi.MRT_BVH_FAST)
     build_s = time.time() - t0
-    dev_ms, rays, paths, clk = time_frames(dist, ctx, scene, sc, opts, steps, warmup, accum=True)
+    dev_ms, rays, paths, clk, _, launches = time_frames(dist, ctx, scene, sc, opts, steps, warmup, accum=True)
     dev_ms = dist.max(dev_ms)
     value = rays * dist.ws / (dev_ms / 1e3) / 1e6
     rays_per_path = rays / paths
@@ -500,7 +510,7 @@ def scene_frame(dist, ctx, name: str, steps: int, warmup: int, args):
             "bvh_build_seconds": build_s,
             "e2e": {"value": rays / steps * dist.ws / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": None, "clocks": clk, "cpu_baseline": cpu}
+            "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -895,7 +905,7 @@ def main():
         emit({**base, "value": rec["value"], "unit": "Mrays/s", "steps": steps, "ms_per_step": rec["ms_per_step"],
               "config": {"workload": rec["workload"], "l2": "flushed before every step (512 MiB write outside the "
                                                              "timed events)"},
-              "e2e": rec["e2e"], "gpu_launches": None, "roofline": None, "clocks": rec["clocks"],
+              "e2e": rec["e2e"], "gpu_launches": rec["gpu_launches"], "roofline": None, "clocks": rec["clocks"],
               "cpu_baseline": rec["cpu_baseline"], args.workload: rec})
         dist.close()
         return

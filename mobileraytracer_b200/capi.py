@@ -99,7 +99,8 @@ class MrtRenderOpts(ctypes.Structure):
 
 class MrtRenderStats(ctypes.Structure):
     _fields_ = [("rays_closest", ctypes.c_uint64), ("rays_shadow", ctypes.c_uint64), ("paths", ctypes.c_uint64),
-                ("device_ms", ctypes.c_float)]
+                ("device_ms", ctypes.c_float), ("trace_ms", ctypes.c_float), ("kernel_launches", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class MrtRasterStats(ctypes.Structure):

@@ -451,12 +451,14 @@ struct CollapseItem {
 
 __device__ __forceinline__ bool rec_internal(const float4 *bin, uint32_t r) { return __float_as_int(bin[2 * (size_t)r + 1].w) == 0; }
 
-#ifndef MRT_COLLAPSE_SMALL
-#define MRT_COLLAPSE_SMALL 1
-#endif
 // The triangles below internal record r when they are at most kMaxLeafTris (a subtree's triangles
-// are contiguous in Morton order): a full wide node keeps such a child as one leaf instead of
-// spending a 128-byte node on two or three children.
+// are contiguous in Morton order): with MRT_COLLAPSE_SMALL a full wide node keeps such a child as one
+// leaf instead of spending a 128-byte node on two or three children.  Off by default: on the
+// 1,000,000-triangle soup it cuts the nodes from 284 k to 176 k and the node visits per camera ray
+// from 29.1 to 25.5 but raises the triangle tests from 1.5 to 7.0, and the frame is 1.3 % slower.
+#ifndef MRT_COLLAPSE_SMALL
+#define MRT_COLLAPSE_SMALL 0
+#endif
 __device__ __forceinline__ bool small_subtree(const float4 *bin, uint32_t n_records, uint32_t r, uint32_t &first,
                                              uint32_t &count) {
     uint32_t st[kMaxLeafTris + 1];

@@ -217,6 +217,8 @@ int mrt_context_create(int device, MrtContext **out) {
     if (st == MRT_OK) st = cuda_status(ctx, cudaMalloc(&ctx->d_counters, 64 * sizeof(uint32_t)), "cudaMalloc");
     if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&ctx->ev0), "event");
     if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&ctx->ev1), "event");
+    for (auto &e : ctx->trace_ev)
+        if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&e), "event");
     for (int k = 0; k < 2 && st == MRT_OK; ++k)
         st = cuda_status(ctx, cudaEventCreateWithFlags(&ctx->wave_ev[k], cudaEventDisableTiming), "event");
     if (st != MRT_OK) {
@@ -239,6 +241,7 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (auto &e : ctx->trace_ev) if (e) cudaEventDestroy(e);
     for (auto &e : ctx->wave_ev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -43,6 +43,8 @@ struct MrtContext {
     int32_t *d_error = nullptr;         // device error flag (MRT_ERR_LIMIT from kernels)
     uint32_t *d_counters = nullptr;     // work counters of the persistent kernels (64 slots)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    static constexpr int kTraceEvents = 16;             // start / end pairs around traversal launches
+    cudaEvent_t trace_ev[2 * kTraceEvents] = {};
     cudaEvent_t wave_ev[2] = {nullptr, nullptr};   // the last two waves of a render (bounded run-ahead)
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];

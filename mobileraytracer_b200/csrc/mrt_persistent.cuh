@@ -20,16 +20,19 @@
 
 namespace mrt {
 
-// the node phase of a warp ends when no lane searches any more, or when fewer than kNodeQuorum lanes
-// search while others hold leaves: those leaves are tested first, and the few searching lanes go on
-// in the next node phase (2 and 4: +2 % on the 1,000,000-triangle soup frame, 8: -2 %)
+// the node phase of a warp ends when no lane searches any more, or when fewer than Q lanes search
+// while others hold leaves: those leaves are tested first, and the few searching lanes go on in the
+// next node phase.  Coherent camera rays (the NoShadows trace) do best with Q = 8 (the 8-wide tree
+// on the 1,000,000-triangle soup frame: 1578 Mrays/s against 1506 at 4 and 1232 at 2), the
+// incoherent rays of the wavefront with Q = 4 (terrain PathTracer: 8 is 1.5 % slower).
 #ifndef MRT_NODE_QUORUM
 #define MRT_NODE_QUORUM 4
 #endif
 constexpr int kNodeQuorum = MRT_NODE_QUORUM;
+template <int Q = kNodeQuorum>
 __device__ __forceinline__ bool node_phase_over(bool searching, bool holding_leaf) {
     const uint32_t s = __ballot_sync(0xFFFFFFFFu, searching);
-    return s == 0u || (__popc(s) < kNodeQuorum && __any_sync(0xFFFFFFFFu, holding_leaf));
+    return s == 0u || (__popc(s) < Q && __any_sync(0xFFFFFFFFu, holding_leaf));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -54,7 +57,7 @@ __device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastT
     trav_begin<kCount>(s, r, len, id, t);   // the plane or sphere hit stays the answer unless a triangle is closer
 }
 
-template <bool kCount, class Work, class Lane, class Stack>
+template <bool kCount, class Work, class Lane, class Stack, int Q = kNodeQuorum>
 __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, Stack &stk) {
     const uint32_t FULL = 0xFFFFFFFFu;
     const int lane_id = threadIdx.x & 31;
@@ -87,7 +90,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, St
         // 2. node phase (lanes holding a leaf step on speculatively while others search)
         for (;;) {
             const bool w = active && trav_wants_node(t);
-            if (node_phase_over(w, active && trav_has_leaf(t))) break;
+            if (node_phase_over<Q>(w, active && trav_has_leaf(t))) break;
             if (w || (active && trav_can_speculate(t))) trav_node_step<kCount>(work.view(lane, s), r, t, stk);
         }
         // 3. leaf phase
@@ -105,10 +108,10 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, St
 }
 
 // the same with the stack in local memory
-template <bool kCount, class Work, class Lane>
+template <bool kCount, int Q = kNodeQuorum, class Work, class Lane>
 __device__ __forceinline__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
     TravStack stk;
-    persistent_closest<kCount>(s, work, lane, stk);
+    persistent_closest<kCount, Work, Lane, TravStack, Q>(s, work, lane, stk);
 }
 
 }  // namespace mrt

@@ -208,6 +208,11 @@ struct NsTraceWork {
 #define MRT_NS_SPLIT 1
 #endif
 constexpr bool kNsSplit = MRT_NS_SPLIT != 0;
+// node-phase quorum of the NoShadows traversal (coherent camera rays)
+#ifndef MRT_NS_QUORUM
+#define MRT_NS_QUORUM 8
+#endif
+constexpr int kNsQuorum = MRT_NS_QUORUM;
 constexpr uint32_t kNsChunk = 1u << 22;
 
 __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, NsTraceWork w, RenderParams p) {
@@ -217,9 +222,9 @@ __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, Ns
         __shared__ uint2 stack_cols[(kNsSmemStack > 0 ? kNsSmemStack : 1) * 128];
         SharedTravStack<(kNsSmemStack > 0 ? kNsSmemStack : 1), 128> stk;
         stk.col = stack_cols + threadIdx.x;
-        persistent_closest<false>(s, w, lane, stk);
+        persistent_closest<false, NsTraceWork, NsTraceLane, decltype(stk), kNsQuorum>(s, w, lane, stk);
     } else {
-        persistent_closest<false>(s, w, lane);
+        persistent_closest<false, kNsQuorum>(s, w, lane);
     }
 }
 
@@ -466,8 +471,9 @@ struct ShadowWork {
 };
 
 // resident blocks of 128 threads per SM for the wavefront's persistent extend and shadow kernels
+// (7 blocks, 72 registers: terrain PathTracer 1387 Mrays/s against 1325 at 8 and 1373 at 6)
 #ifndef MRT_WAVE_BLOCKS_PER_SM
-#define MRT_WAVE_BLOCKS_PER_SM 8
+#define MRT_WAVE_BLOCKS_PER_SM 7
 #endif
 constexpr int kWaveBlocksPerSm = MRT_WAVE_BLOCKS_PER_SM;
 
@@ -776,7 +782,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     }
     if (plan.round_first.size() > 1 && o->spp > 1) {
         // pixels revisited within a pass: the reference's pass-major order, one pass at a time
-        MrtRenderStats total{0, 0, 0, 0.0f};
+        MrtRenderStats total{0, 0, 0, 0.0f, 0.0f, 0u, 0u};
         for (uint32_t si = 0; si < o->spp; ++si) {
             MrtRenderOpts one = *o;
             one.spp = 1;
@@ -788,6 +794,8 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             total.rays_shadow += part.rays_shadow;
             total.paths += part.paths;
             total.device_ms += part.device_ms;
+            total.trace_ms += part.trace_ms;
+            total.kernel_launches += part.kernel_launches;
         }
         if (stats) *stats = total;
         return MRT_OK;
@@ -795,6 +803,17 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     const int accel = s->opts.accelerator, mode = s->opts.bvh_mode;
     const int grid = ctx->sm_count * 16;
     uint64_t rays_closest = 0, rays_shadow = 0;
+    uint32_t launches = 0;   // kernels launched by this render
+    float trace_ms = 0.0f;
+    int trace_pairs = 0;   // recorded pairs of ctx->trace_ev not yet added to trace_ms
+    auto add_trace_time = [&]() {
+        if (trace_pairs > 0 && cudaEventSynchronize(ctx->trace_ev[2 * trace_pairs - 1]) == cudaSuccess)
+            for (int k = 0; k < trace_pairs; ++k) {
+                float t = 0.0f;
+                if (cudaEventElapsedTime(&t, ctx->trace_ev[2 * k], ctx->trace_ev[2 * k + 1]) == cudaSuccess) trace_ms += t;
+            }
+        trace_pairs = 0;
+    };
     s->progress.store(0);
     cudaEventRecord(ctx->ev0, q);
     if (direct_shader(o->shader)) {
@@ -818,7 +837,12 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                         const uint32_t n_s = std::min(per, o->spp - s0);
                         NsTraceWork tw{nullptr, plan.round_first[r], j0, n_pix, s0, n_pix * n_s, tiles_x, ctx->d_counters, hits};
                         cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
+                        if (trace_pairs == MrtContext::kTraceEvents) add_trace_time();
+                        cudaEventRecord(ctx->trace_ev[2 * trace_pairs], q);
                         k_ns_trace<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, tw, p);
+                        cudaEventRecord(ctx->trace_ev[2 * trace_pairs + 1], q);
+                        ++trace_pairs;
+                        launches += 2;
                         k_ns_shade<<<(n_pix + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0, n_pix, s0, n_s,
                                                                         tiles_x, hits);
                     }
@@ -827,12 +851,15 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_fast<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
+                ++launches;
             } else if (accel == MRT_ACCEL_REGULAR_GRID) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_grid<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
+                ++launches;
             } else {
                 MRT_DISPATCH(launch_noshadows, accel, mode, s->dev, p, plan.round_first[r], plan.round_count[r], grid, q);
+                ++launches;
             }
         }
         rays_closest = (uint64_t)plan.n_tasks * o->spp;
@@ -893,6 +920,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 if (paths) {
                     cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                     k_wave_paths<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, w, ctx->d_counters);
+                    launches += 2;   // with the fold below
                 } else {
                     cudaMemsetAsync(w.levels, 0, sizeof(Level) * (levels + 2), q);
                     cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t) * 2 * (levels + 1), q);
@@ -900,6 +928,8 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                     for (int b = 0; b < levels; ++b)
                         MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, ctx->d_counters);
                     for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
+                    launches += 2u + 4u * (uint32_t)levels;   // raygen, per level extend / shade / shadow /
+                                                              // resolve, the fold below
                 }
                 k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
                 const int slot = (int)(waves_issued % 2);
@@ -919,6 +949,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
     if (st == MRT_OK) st = cuda_status(ctx, cudaEventSynchronize(ctx->ev1), "render");
     if (st == MRT_OK) st = check_kernel_error(ctx);
     s->progress.store(o->spp);
+    add_trace_time();
     if (stats) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -926,6 +957,9 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         stats->rays_shadow = rays_shadow;
         stats->paths = (uint64_t)plan.n_tasks * o->spp;
         stats->device_ms = ms;
+        stats->trace_ms = trace_ms;
+        stats->kernel_launches = launches;
+        stats->reserved = 0;
     }
     return st;
 }
@@ -1118,9 +1152,11 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
     const int accel = s->opts.accelerator, mode = s->opts.bvh_mode;
     const int grid = ctx->sm_count * 16;
     uint64_t rays_closest = 0, rays_shadow = 0;
+    uint32_t launches = 0;
     s->progress.store(0);
     cudaEventRecord(ctx->ev0, q);
     if (direct_shader(o->shader)) {
+        launches = 1;
         if (accel == MRT_ACCEL_BVH && mode == MRT_BVH_FAST) {
             const uint32_t tiles_x = o->width / 2u;   // width is a multiple of 16, rows of 16
             cudaMemsetAsync(counters, 0, sizeof(uint32_t), q);
@@ -1161,6 +1197,7 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
             for (int b = 0; b < levels; ++b) MRT_DISPATCH(launch_wave_level, accel, mode, s->dev, p, w, b, grid, q, counters);
             for (int b = levels - 1; b >= 0; --b) k_wave_resolve<<<grid, 128, 0, q>>>(s->dev, p, w, b);
             k_wave_accumulate<<<grid, 128, 0, q>>>(p, w);
+            launches += 2u + 4u * (uint32_t)levels;
             const int slot = (int)(waves_issued % 2);
             cudaEventRecord(ctx->wave_ev[slot], q);
             done_samples[slot] = (r0 + w.n_roots) / std::max<uint64_t>(1, p.n_tasks);
@@ -1184,6 +1221,9 @@ extern "C" int mrt_render_noalloc(MrtScene *s, const MrtCamera *cam, const MrtRe
         stats->rays_shadow = rays_shadow;
         stats->paths = (uint64_t)p.n_tasks * o->spp;
         stats->device_ms = ms;
+        stats->trace_ms = 0.0f;
+        stats->kernel_launches = launches;
+        stats->reserved = 0;
     }
     return st;
 }
