@@ -220,8 +220,8 @@ typedef struct MrtRenderStats {
     uint64_t paths;         /* camera paths (pixel samples) */
     float device_ms;        /* device time of the render */
     float trace_ms;         /* of which the closest-hit traversal launches of a NoShadows / DepthMap /
-                               DiffuseMaterial frame on the FAST BVH (the rest is shading and the
-                               running mean); 0 for other renders */
+                               DiffuseMaterial frame on the FAST BVH or the RegularGrid (the rest is
+                               shading and the running mean); 0 for other renders */
     uint32_t kernel_launches;  /* kernels the render launched */
     uint32_t reserved;
 } MrtRenderStats;

@@ -233,8 +233,15 @@ __global__ void __launch_bounds__(128, 8) k_batch_paths(BatchState b) {
     persistent_paths(work);
 }
 
+// threads per SM the batch's traversal kernels are compiled for (registers per thread: 65536 / this);
+// the 256-job batch: 1030 Mrays/s at 768, 1024 at 896, 998 at 1024 (spills at 64 registers)
+#ifndef MRT_BATCH_THREADS_PER_SM
+#define MRT_BATCH_THREADS_PER_SM 768
+#endif
+constexpr int kBatchThreadsPerSm = MRT_BATCH_THREADS_PER_SM;
+
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_extend(BatchState b, int level) {
+__global__ void __launch_bounds__(kBlock, kBatchThreadsPerSm / kBlock) k_batch_extend(BatchState b, int level) {
     Level L = b.levels[level];
     L.start = min(L.start, b.ray_cap);
     L.count = min(L.count, b.ray_cap - L.start);
@@ -248,7 +255,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_extend(BatchSta
 }
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_batch_shadow(BatchState b, int level) {
+__global__ void __launch_bounds__(kBlock, kBatchThreadsPerSm / kBlock) k_batch_shadow(BatchState b, int level) {
     const uint32_t n = min(b.levels[level].shadow_count, b.shadow_cap);
     BatchShadowWork work{b, n, b.work + 2 * level + 1};
     BatchLane lane;

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(128, 8) k_trace_persistent(DevScene s, TraceWo
     persistent_closest<kCount>(s, work, lane);
 }
 
-__global__ void __launch_bounds__(128, 8) k_trace_grid_persistent(DevScene s, TraceWork<false> work) {
+__global__ void __launch_bounds__(128, kGridBlocksPerSm) k_trace_grid_persistent(DevScene s, TraceWork<false> work) {
     TraceLane lane;
     persistent_grid_closest(s, work, lane);
 }

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_render_noshadows_fast(D
 
 // the same work on the RegularGrid: the persistent grid walk (mrt_gridwalk.cuh), one cell per lane
 // and loop iteration
-__global__ void __launch_bounds__(128, 8) k_render_noshadows_grid(DevScene s, RenderParams p, uint32_t first,
+__global__ void __launch_bounds__(128, kGridBlocksPerSm) k_render_noshadows_grid(DevScene s, RenderParams p, uint32_t first,
                                                                uint32_t count, uint32_t *ctr, uint32_t tiles_x) {
     NsWork w{&s, &p, first, count, ctr, tiles_x};
     NsLane lane;
@@ -226,6 +226,13 @@ __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, Ns
     } else {
         persistent_closest<false, kNsQuorum>(s, w, lane);
     }
+}
+
+// the same traversal pass on the RegularGrid (the persistent grid walk)
+__global__ void __launch_bounds__(128, kGridBlocksPerSm) k_ns_trace_grid(DevScene s, NsTraceWork w, RenderParams p) {
+    w.p = &p;
+    NsTraceLane lane;
+    persistent_grid_closest(s, w, lane);
 }
 
 __global__ void __launch_bounds__(128) k_ns_shade(DevScene s, RenderParams p, uint32_t first, uint32_t j0, uint32_t n_pix,
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(128, kWaveBlocksPerSm) k_wave_extend_fast(DevS
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
-__global__ void __launch_bounds__(128, 8) k_wave_extend_grid(DevScene s, WaveState w, int level, uint32_t *ctr) {
+__global__ void __launch_bounds__(128, kGridBlocksPerSm) k_wave_extend_grid(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const Level L = clamp_level(w, w.levels[level]);
     ExtendWork work{w, L, ctr};
     WaveLane lane;
@@ -822,7 +829,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
         const uint32_t tiles_x = (plan.implicit && o->width % 2u == 0 && rows % 16u == 0) ? o->width / 2u : 0u;
         for (size_t r = 0; r < plan.round_first.size(); ++r) {
             if (s->stop.load()) return cancelled(ctx, q);
-            if (fast && kNsSplit) {
+            if ((fast || accel == MRT_ACCEL_REGULAR_GRID) && kNsSplit) {
                 // chunks of at most kNsChunk (sample, pixel) items: whole samples of up to kNsChunk pixels
                 const uint32_t count = plan.round_count[r];
                 const uint32_t n_pix_max = std::min<uint32_t>(count, kNsChunk);
@@ -839,7 +846,8 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                         cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                         if (trace_pairs == MrtContext::kTraceEvents) add_trace_time();
                         cudaEventRecord(ctx->trace_ev[2 * trace_pairs], q);
-                        k_ns_trace<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, tw, p);
+                        if (fast) k_ns_trace<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, tw, p);
+                        else k_ns_trace_grid<<<ctx->sm_count * kGridBlocksPerSm, 128, 0, q>>>(s->dev, tw, p);
                         cudaEventRecord(ctx->trace_ev[2 * trace_pairs + 1], q);
                         ++trace_pairs;
                         launches += 2;
@@ -854,7 +862,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                 ++launches;
             } else if (accel == MRT_ACCEL_REGULAR_GRID) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
-                k_render_noshadows_grid<<<ctx->sm_count * 8, 128, 0, q>>>(s->dev, p, plan.round_first[r],
+                k_render_noshadows_grid<<<ctx->sm_count * kGridBlocksPerSm, 128, 0, q>>>(s->dev, p, plan.round_first[r],
                                                                          plan.round_count[r], ctx->d_counters, tiles_x);
                 ++launches;
             } else {
