@@ -42,6 +42,7 @@ FRAME = "NoShadows 1920x1080 1 spp, 1,000,000-triangle soup seed 0, 1 point ligh
 WORKLOAD = FRAME + ", FAST BVH built on the device"
 REF_WORKLOAD = FRAME + ", the reference's BVH (BVH<Triangle>, top-down SAH) built on the host"
 PROFILE = os.path.join(ROOT, "profiles", "ns_trace_soup_1080p.md")
+GRID_PROFILE = os.path.join(ROOT, "profiles", "ns_trace_grid_soup_1080p.md")
 FAST_NODE_BYTES = 128  # bytes of one 8-wide node, the unit of the FAST tree's counting replay
 
 
@@ -414,22 +415,23 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
     n_hit = int(np.sum((hits["id"] >> 30) == capi.MRT_PRIM_TRIANGLE))
     peak, peak_kind = measured_peak()
     n_nodes, n_tris = int(nodes.sum(dtype=np.int64)), int(tris.sum(dtype=np.int64))
+    shade = {"name": "k_ns_shade (per pixel: hit record 8 + triangle record 48 + shading 76 per hit + bitmap 8)",
+             "algorithmic_bytes_per_launch": 16 * len(rays_np) + (48 + 76) * n_hit, "ms": ms - trace_ms}
     if accel == capi.MRT_ACCEL_REGULAR_GRID:
-        # result 8 + cells 8 (start[c], start[c + 1]) + per reference 4 (index) + 48 (A, AB, AC) + shading 76
-        alg = 8 * len(rays_np) + 8 * n_nodes + 52 * n_tris + 76 * n_hit
-        counts = {"cells_per_ray": n_nodes / len(rays_np), "refs_per_ray": n_tris / len(rays_np)}
-        kernel = "k_render_noshadows_grid (persistent grid walk)"
+        # the traversal kernel: cells 8 (start[c], start[c + 1]) + per reference 4 (index) + 48 (A, AB, AC)
+        # + the 8-byte hit record written
+        alg = 8 * len(rays_np) + 8 * n_nodes + 52 * n_tris
+        counts = {"cells_per_ray": n_nodes / len(rays_np), "refs_per_ray": n_tris / len(rays_np),
+                  "kernel_ms": trace_ms, "frame_ms": ms, "shade_kernel": shade}
+        kernel = "k_ns_trace_grid (persistent grid walk; k_ns_shade shades the frame's samples after it)"
     else:
         # the traversal kernel: node bytes + 48 per triangle record + the 8-byte hit record written
         alg = FAST_NODE_BYTES * n_nodes + 48 * n_tris + 8 * len(rays_np)
         counts = {"node_fetches_per_ray": n_nodes / len(rays_np), "node_fetch_bytes": FAST_NODE_BYTES,
                   "tri_records_per_ray": n_tris / len(rays_np), "kernel_ms": trace_ms, "frame_ms": ms,
-                  "shade_kernel": {"name": "k_ns_shade (per pixel: hit record 8 + triangle record 48 + shading 76 "
-                                           "per hit + bitmap 8)",
-                                   "algorithmic_bytes_per_launch": 16 * len(rays_np) + (48 + 76) * n_hit,
-                                   "ms": ms - trace_ms}}
+                  "shade_kernel": shade}
         kernel = "k_ns_trace (persistent traversal; k_ns_shade shades the frame's samples after it)"
-    kernel_ms = trace_ms if (accel != capi.MRT_ACCEL_REGULAR_GRID and trace_ms > 0) else ms
+    kernel_ms = trace_ms if trace_ms > 0 else ms
     achieved = alg / (kernel_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
@@ -939,7 +941,7 @@ def main():
     sc = make_soup()
     ctx = m.Context(dist.local)
     if args.workload == "grid":
-        rec = soup_frame(dist, ctx, sc, args, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST)
+        rec = soup_frame(dist, ctx, sc, args, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST, profile=GRID_PROFILE)
         emit({**base, "value": rec["value"], "unit": "Mrays/s", "ms_per_step": rec["ms_per_step"],
               "config": {"workload": FRAME + ", RegularGrid G = 128 (the reference's sizing rule)"},
               **{k: rec[k] for k in ("e2e", "gpu_launches", "roofline", "clocks", "cpu_baseline")}})
@@ -957,7 +959,7 @@ def main():
     if args.workload == "all":
         configs = {}
         t_all = time.time()
-        g128 = soup_frame(dist, ctx, sc, args, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST)
+        g128 = soup_frame(dist, ctx, sc, args, capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST, profile=GRID_PROFILE)
         configs["soup_1080p_grid_G128"] = {"workload": FRAME + ", RegularGrid with G = 128 by the reference's "
                                                                "sizing rule (Shader.cpp:76-105), reference cell indexing",
                                            **g128}
