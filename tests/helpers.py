@@ -56,3 +56,29 @@ def near_tie_mask(rays: np.ndarray, a: np.ndarray, b: np.ndarray, rel: float = 1
     both = (a["id"] != capi.MRT_HIT_NONE) & (b["id"] != capi.MRT_HIT_NONE)
     ta, tb = a["t"].astype(np.float64), b["t"].astype(np.float64)
     return both & (np.abs(ta - tb) <= rel * np.maximum(np.abs(ta), np.abs(tb)))
+
+
+def near_guard_corner_scene(seed: int = 11, per_corner: int = 40, w: int = 160, h: int = 120):
+    """Triangles with one vertex within 1e-4 (relative) of a corner where the near plane (0.1) meets
+    the raster preview's guard band (16 viewports) for a camera at the origin looking along +z with a
+    45-degree vertical field of view, the other vertices in front of and behind the near plane: the
+    clipper meets near-coincident planes, where rounded intersection points can add vertices."""
+    from mobileraytracer_b200 import scenes
+    rng = np.random.default_rng(seed)
+    cam = scenes.camera((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 60.0, 45.0)
+    t = np.tan(np.radians(0.918 * 45.0) / 2.0)
+    tris = []
+    for sx in (-1.0, 1.0):
+        for sy in (-1.0, 1.0):
+            corner = np.array([sx * 16.0 * 0.1 * t * w / h, sy * 16.0 * 0.1 * t, 0.1])
+            for _ in range(per_corner):
+                a = corner * (1.0 + rng.uniform(-1e-4, 1e-4, 3))
+                b = rng.uniform([-2.0, -2.0, 0.5], [2.0, 2.0, 5.0])
+                c = rng.uniform([-2.0, -2.0, -1.0], [2.0, 2.0, 0.05])
+                tris.append([*a, *b, *c] if rng.random() < 0.5 else [*a, *c, *b])
+    sc = scenes.Scene()
+    sc.tri_abc = np.asarray(tris, np.float32)
+    n = len(tris)
+    sc.tri_material = np.full(n, -1, np.int32)
+    sc.tri_colors = rng.uniform(0.1, 1.0, (n, 9)).astype(np.float32)
+    return sc, cam, w, h

@@ -4,6 +4,7 @@
   (the persistent kernel the benchmark times) against the oracle's exact closest hit, on every
   97th pixel of the rows the block schedule renders (0..1071), plus the untouched rows 1072..1079
   (Renderer.cpp:20-21).
+* The same frame on the RegularGrid (G = 128) against the oracle's reference walk.
 * The reference BVH (BVH<Triangle>::trace, BVH.hpp:158-213, compiled from the reference sources) on
   the same camera rays: every ray where its closest hit differs from the exact one is classified
   (a box its slab test rejects although a closer triangle inside passes the reference's own
@@ -73,6 +74,28 @@ def test_soup_1080p_frame_through_the_timed_kernel(ctx, soup, soup_subset):
     nd = int(np.sum(bm[ys, xs] != want))
     assert nd == 0, f"{nd} of {len(want)} pixels differ"
     assert np.count_nonzero(bm[ys, xs] & 0xFFFFFF) > len(want) // 4   # the soup covers the frame's middle
+
+
+def test_soup_1080p_frame_on_the_grid(ctx, soup, soup_subset):
+    """The same frame on the RegularGrid at the reference's G = 128 (the grid trace and shade kernels the
+    benchmark times): every 97th pixel equals the oracle's reference walk bit for bit."""
+    import torch
+    opts = capi.render_opts(shader=capi.MRT_SHADER_NOSHADOWS, width=W, height=H, spp=1, spl=1)
+    g = Scene(ctx, soup).build(capi.MRT_ACCEL_REGULAR_GRID, capi.MRT_BVH_FAST)
+    assert g.accel_info()["grid_size"] == 128
+    bm = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(H * W * 4, dtype=torch.float32, device="cuda")
+    _, _, st = g.render(soup.camera, opts, bitmap=bm, accum=acc)
+    assert st.kernel_launches == 2 and 0.0 < st.trace_ms <= st.device_ms
+    bm = bm.cpu().numpy().view(np.uint32).reshape(H, W)
+    acc = acc.cpu().numpy().reshape(H, W, 4)
+    o = O.OrcScene(soup, capi.MRT_ACCEL_REGULAR_GRID, camera_position=list(soup.camera.position))
+    xy = np.stack([soup_subset % W, soup_subset // W], 1).astype(np.uint32)
+    vals = o.render_pixels(soup.camera, opts, xy, threads=os.cpu_count() or 8)[:, 0, :]
+    ys, xs = soup_subset // W, soup_subset % W
+    assert np.array_equal(acc[ys, xs, :3].view(np.uint32), vals.view(np.uint32))
+    want = _expected_bitmap(vals, np.zeros(len(vals), np.uint32))
+    assert int(np.sum(bm[ys, xs] != want)) == 0
 
 
 def test_reference_bvh_disagreements_on_the_1080p_rays(ctx, soup, soup_subset):

@@ -108,6 +108,14 @@ def test_pixel_centre_edges_and_guard_band(ctx):
     assert st.fragments == 40 * 30
 
 
+def test_vertices_at_near_plane_and_guard_band_corners(ctx):
+    # one vertex of every triangle at a corner of the near plane and the guard band: the device clipper
+    # equals the restatement bit for bit (bitmap, drawn triangles, covered samples)
+    from helpers import near_guard_corner_scene
+    sc, cam, w, h = near_guard_corner_scene()
+    _check(ctx, sc, cam, w, h)
+
+
 def test_full_queue_sends_triangles_to_further_passes(ctx, monkeypatch):
     """Large pieces beyond the queue's room: the triangles owning them are drawn whole by further
     passes over an overflow list.  With the room lowered to 14 entries (the pieces of one clipped

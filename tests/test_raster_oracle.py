@@ -130,3 +130,13 @@ def test_edges_through_pixel_centres_are_owned_once():
     assert drawn == 4
     assert frags == int((bm != 0).sum())   # every covered centre belongs to exactly one triangle
     assert frags == 31 * 31                # the square's centres, edges included once
+
+
+def test_vertices_at_near_plane_and_guard_band_corners():
+    # near-coincident clip planes: the clipper's polygon stays within its bound and the triangles
+    # that reach the view are drawn
+    from helpers import near_guard_corner_scene
+    sc, cam, w, h = near_guard_corner_scene()
+    bm, drawn, frags = preview(sc, w, h, cam)
+    assert 0 < drawn <= sc.n_triangles and frags >= int((bm != 0).sum()) > 0   # frags: covered samples, overdraw included
+
