@@ -596,26 +596,26 @@ __global__ void k_collapse(const float4 *__restrict__ bin, uint32_t n_records, c
     w[1] = __float_as_uint(nlo.y);
     w[2] = __float_as_uint(nlo.z);
     w[3] = (uint32_t)(ex + 127) | ((uint32_t)(ey + 127) << 8) | ((uint32_t)(ez + 127) << 16) | (imask << 24);
-    w[4] = child_base;
-    w[5] = tri_base;
-    w[6] = w[7] = 0;
+    w[kNodeChildBase] = child_base;
+    w[kNodeTriBase] = tri_base;
+    w[kNodeMeta] = w[kNodeMeta + 1] = 0;
     uint32_t offset = 0, rank = 0;
     for (int sl = 0; sl < kWide; ++sl) {
         const int k = child_at[sl];
         if (k < 0) {   // empty slot: an inverted box, no meta
-            w[8 + sl] = w[16 + sl] = w[24 + sl] = 0xFFFFu;
+            w[node_plane_word(0, sl)] = w[node_plane_word(1, sl)] = w[node_plane_word(2, sl)] = 0xFFFFu;
             continue;
         }
-        w[8 + sl] = quantise(nlo.x, sx, lo[k].x, hi[k].x);
-        w[16 + sl] = quantise(nlo.y, sy, lo[k].y, hi[k].y);
-        w[24 + sl] = quantise(nlo.z, sz, lo[k].z, hi[k].z);
+        w[node_plane_word(0, sl)] = quantise(nlo.x, sx, lo[k].x, hi[k].x);
+        w[node_plane_word(1, sl)] = quantise(nlo.y, sy, lo[k].y, hi[k].y);
+        w[node_plane_word(2, sl)] = quantise(nlo.z, sz, lo[k].z, hi[k].z);
         if ((imask >> sl) & 1u) {
             out[qpos + rank] = CollapseItem{__float_as_uint(lo[k].w), 2u, child_base + rank};
             ++rank;
         } else {
             const uint32_t first = __float_as_uint(lo[k].w), count = (uint32_t)__float_as_int(hi[k].w);
             if (count == 0 || count > kMaxLeafTris || (uint64_t)first + count > n_tri) { atomicMax(&ctrs[2], 1u); return; }
-            w[6 + (sl >> 2)] |= ((((1u << count) - 1u) << 5) | offset) << (8 * (sl & 3));
+            w[kNodeMeta + (sl >> 2)] |= ((((1u << count) - 1u) << 5) | offset) << (8 * (sl & 3));
             for (uint32_t j = 0; j < count; ++j)
                 for (int c = 0; c < 3; ++c) tris[3 * (size_t)(tri_base + offset + j) + c] = mtris[3 * (size_t)(first + j) + c];
             offset += count;

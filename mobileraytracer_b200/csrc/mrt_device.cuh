@@ -20,6 +20,12 @@ constexpr float kEpsilon = 1.0e-06f;        // Utils.hpp:37
 constexpr float kRayLengthMax = 1.0e+30f;   // Utils.hpp:33
 constexpr int kWide = 8;                    // children per node of the FAST tree
 constexpr int kNodeWords = 32;              // 32-bit words per node of the FAST tree (128 bytes)
+// Word positions in a FAST node.  Each 64-byte half holds what the test of four children reads: the
+// first the grid origin (words 0-2), the grid exponents and internal-child mask (3) and the planes of
+// slots 0-3, the second the first internal child's node index (16), the first leaf triangle's record
+// index (17), the leaf meta bytes of slots 0-3 and 4-7 (18, 19) and the planes of slots 4-7.
+constexpr int kNodeChildBase = 16, kNodeTriBase = 17, kNodeMeta = 18;
+__host__ __device__ constexpr int node_plane_word(int axis, int slot) { return (slot < 4 ? 4 : 20) + 4 * axis + (slot & 3); }
 constexpr uint32_t kMaxLeafTris = 3;        // triangles per leaf child of the FAST tree
 constexpr uint32_t kMaxFastTris = 1u << 27; // triangles of one FAST tree (indices and counts stay in 32 bits)
 constexpr float kSphereEpsilon = 1.0e-05f;  // Sphere.cpp:43,50

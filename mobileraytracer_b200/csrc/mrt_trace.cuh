@@ -347,16 +347,19 @@ __device__ bool grid_occ(const DevScene &s, const Ray &r, float dist) {
 // and Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017);
 // here the boxes are quantised to 16 bits and every plane distance is bounded by directed rounding.
 //
-// Node, 32 words (the fnodes array holds n_fnodes of them):
+// Node, 32 words (the fnodes array holds n_fnodes of them), in two 64-byte halves that each hold what
+// the test of four children reads (word positions: kNodeChildBase, kNodeTriBase, kNodeMeta and
+// node_plane_word() in mrt_device.cuh):
 //   w[0..2]  origin p of the quantisation grid (floats)
 //   w[3]     ex | ey << 8 | ez << 16 (axis a's grid step is 2^(e_a - 127)) | imask << 24 (slots
 //            holding internal children)
-//   w[4]     child base: node index of the first internal child
-//   w[5]     triangle base: record index of the first triangle of the leaf children
-//   w[6..7]  one byte per slot: a leaf child's triangle bits (1, 3 or 7 for 1..3 triangles) << 5 | the
+//   w[4..15] slots 0-3's box on x (w[4..7]), y (w[8..11]), z (w[12..15]): qlo | qhi << 16, the planes
+//            p + step * q; the quantised box contains the exact box of everything below the slot
+//   w[16]    child base: node index of the first internal child
+//   w[17]    triangle base: record index of the first triangle of the leaf children
+//   w[18..19] one byte per slot: a leaf child's triangle bits (1, 3 or 7 for 1..3 triangles) << 5 | the
 //            offset of its first triangle from the triangle base; 0 for internal and empty slots
-//   w[8+k], w[16+k], w[24+k]   slot k's box on x, y, z: qlo | qhi << 16, the planes p + step * q;
-//            the quantised box contains the exact box of everything below the slot
+//   w[20..31] slots 4-7's box on x, y, z as w[4..15]
 // Slots are assigned by the octant of the child's centre within the node, so visiting the children
 // in the order slot ^ octant(ray direction) is close to front to back.
 // ---------------------------------------------------------------------------------------------
@@ -432,10 +435,47 @@ __device__ __forceinline__ uint32_t slots_to_keys(uint32_t m, uint32_t oct) {
     return m;
 }
 
+// 32 bytes at a 32-byte-aligned address as one load (sm_100: 256-bit loads), through the read-only path
+#ifndef MRT_NODE_LDG256
+#define MRT_NODE_LDG256 1
+#endif
+__device__ __forceinline__ void ldg_32b(const uint4 *p, uint4 &a, uint4 &b) {
+#if MRT_NODE_LDG256
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p));
+#else
+    a = __ldg(p);
+    b = __ldg(p + 1);
+#endif
+}
+
+// the four children of one half-node (planes x, y, z of slots 4h..4h+3) against the ray: bit k of the
+// result is slot 4h + k's box possibly touched
+__device__ __forceinline__ uint32_t half_hits(const uint4 &xq, const uint4 &yq, const uint4 &zq, float ax, float ay,
+                                              float az, float lox, float loy, float loz, float hix, float hiy,
+                                              float hiz, uint32_t nx, uint32_t ny, uint32_t nz, float tmax) {
+    uint32_t hits = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t wx = uint4_word(xq, j), wy = uint4_word(yq, j), wz = uint4_word(zq, j);
+        const float tnx = __fmaf_rd(grid_offset(wx, nx), ax, lox), tfx = __fmaf_ru(grid_offset(wx, nx ^ 0x22u), ax, hix);
+        const float tny = __fmaf_rd(grid_offset(wy, ny), ay, loy), tfy = __fmaf_ru(grid_offset(wy, ny ^ 0x22u), ay, hiy);
+        const float tnz = __fmaf_rd(grid_offset(wz, nz), az, loz), tfz = __fmaf_ru(grid_offset(wz, nz ^ 0x22u), az, hiz);
+        const float tn = max3f(tnx, tny, fmaxf(tnz, 0.0f));
+        const float tf = min3f(tfx, tfy, fminf(tfz, tmax));
+        if (tn <= tf * 1.000001f) hits |= 1u << j;
+    }
+    return hits;
+}
+
 template <class S>
 __device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const FastRay &f, const V3 &o, float tmax) {
     const uint4 *p = reinterpret_cast<const uint4 *>(s.fnodes) + (size_t)node * (kNodeWords / 4);
-    const uint4 h0 = __ldg(p), h1 = __ldg(p + 1);
+    // first half: grid origin, exponents and internal mask; planes of slots 0-3 on x, y, z
+    uint4 h0, x0, y0, z0;
+    ldg_32b(p, h0, x0);
+    ldg_32b(p + 2, y0, z0);
     // per axis: A = step / d, and bounds of (p - o) / d - 2^23 A
     const float ax = __uint_as_float((h0.w & 0xFFu) << 23) * f.inv.x;
     const float ay = __uint_as_float(((h0.w >> 8) & 0xFFu) << 23) * f.inv.y;
@@ -451,22 +491,12 @@ __device__ __forceinline__ NodeHits node_hits(const S &s, uint32_t node, const F
     const uint32_t ny = 0x7410u + ((f.oct & 2u) ? 0x22u : 0u);
     const uint32_t nz = 0x7410u + ((f.oct & 4u) ? 0x22u : 0u);
     const uint32_t imask = h0.w >> 24;
-    uint32_t hits = 0;   // slot k's box may be touched: bit k
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {   // four children at a time: fewer registers live
-        const uint4 xq = __ldg(p + 2 + half), yq = __ldg(p + 4 + half), zq = __ldg(p + 6 + half);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int k = 4 * half + j;
-            const uint32_t wx = uint4_word(xq, j), wy = uint4_word(yq, j), wz = uint4_word(zq, j);
-            const float tnx = __fmaf_rd(grid_offset(wx, nx), ax, lox), tfx = __fmaf_ru(grid_offset(wx, nx ^ 0x22u), ax, hix);
-            const float tny = __fmaf_rd(grid_offset(wy, ny), ay, loy), tfy = __fmaf_ru(grid_offset(wy, ny ^ 0x22u), ay, hiy);
-            const float tnz = __fmaf_rd(grid_offset(wz, nz), az, loz), tfz = __fmaf_ru(grid_offset(wz, nz ^ 0x22u), az, hiz);
-            const float tn = max3f(tnx, tny, fmaxf(tnz, 0.0f));
-            const float tf = min3f(tfx, tfy, fminf(tfz, tmax));
-            if (tn <= tf * 1.000001f) hits |= 1u << k;
-        }
-    }
+    uint32_t hits = half_hits(x0, y0, z0, ax, ay, az, lox, loy, loz, hix, hiy, hiz, nx, ny, nz, tmax);
+    // second half: child base, triangle base, leaf meta bytes; planes of slots 4-7
+    uint4 h1, x1, y1, z1;
+    ldg_32b(p + 4, h1, x1);
+    ldg_32b(p + 6, y1, z1);
+    hits |= half_hits(x1, y1, z1, ax, ay, az, lox, loy, loz, hix, hiy, hiz, nx, ny, nz, tmax) << 4;
     // the triangles of the leaf children hit (meta byte k: triangle bits << 5 | offset)
     uint32_t tris = 0;
     for (uint32_t lh = hits & ~imask; lh; lh &= lh - 1u) {

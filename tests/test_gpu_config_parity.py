@@ -1,7 +1,7 @@
 """Parity at the sizes the benchmarks time (GPU).
 
 * The 1920x1080 NoShadows frame of the 1,000,000-triangle soup through mrt_render on the FAST BVH
-  (the persistent kernel the benchmark times) against the oracle's exact closest hit, on every
+  (the trace and shade kernels the benchmark times) against the oracle's exact closest hit, on every
   97th pixel of the rows the block schedule renders (0..1071), plus the untouched rows 1072..1079
   (Renderer.cpp:20-21).
 * The same frame on the RegularGrid (G = 128) against the oracle's reference walk.
