@@ -240,14 +240,14 @@ __global__ void __launch_bounds__(128, 8) k_batch_paths(BatchState b) {
 #endif
 constexpr int kBatchThreadsPerSm = MRT_BATCH_THREADS_PER_SM;
 
-template <int kBlock>
+template <int kBlock, int Q>
 __global__ void __launch_bounds__(kBlock, kBatchThreadsPerSm / kBlock) k_batch_extend(BatchState b, int level) {
     Level L = b.levels[level];
     L.start = min(L.start, b.ray_cap);
     L.count = min(L.count, b.ray_cap - L.start);
     BatchExtendWork work{b, L, b.work + 2 * level};
     BatchLane lane;
-    persistent_closest<false>(b.scenes[0], work, lane);
+    persistent_closest<false, Q>(b.scenes[0], work, lane);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (!b.desc->dry) atomicAdd(&b.counters[0], (unsigned long long)L.count);
         atomicAdd(&b.counters[2], (unsigned long long)L.count);
@@ -474,7 +474,8 @@ BatchState state_of(MrtBatch *b, int pipe) {
 
 template <int kBlock>
 void launch_traversal(const BatchState &s, int level, int grid, cudaStream_t q, bool extend) {
-    if (extend) k_batch_extend<kBlock><<<grid, kBlock, 0, q>>>(s, level);
+    if (extend && level == 0) k_batch_extend<kBlock, kCameraQuorum><<<grid, kBlock, 0, q>>>(s, level);   // camera rays
+    else if (extend) k_batch_extend<kBlock, kNodeQuorum><<<grid, kBlock, 0, q>>>(s, level);
     else k_batch_shadow<kBlock><<<grid, kBlock, 0, q>>>(s, level);
 }
 

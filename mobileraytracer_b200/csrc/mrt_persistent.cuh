@@ -22,13 +22,18 @@ namespace mrt {
 
 // the node phase of a warp ends when no lane searches any more, or when fewer than Q lanes search
 // while others hold leaves: those leaves are tested first, and the few searching lanes go on in the
-// next node phase.  Coherent camera rays (the NoShadows trace) do best with Q = 8 (the 8-wide tree
-// on the 1,000,000-triangle soup frame: 1578 Mrays/s against 1506 at 4 and 1232 at 2), the
-// incoherent rays of the wavefront with Q = 4 (terrain PathTracer: 8 is 1.5 % slower).
+// next node phase.  Coherent camera rays do best with Q = 16 (the NoShadows trace of the
+// 1,000,000-triangle soup frame: 1757 Mrays/s against 1757 at 20, 1715 at 24, 1575 at 32, 1610 at
+// 8), the incoherent bounces of the wavefront with Q = 4 (terrain PathTracer: 3, 4 and 6 within
+// 0.3 %, 8 1.5 % slower).
 #ifndef MRT_NODE_QUORUM
 #define MRT_NODE_QUORUM 4
 #endif
 constexpr int kNodeQuorum = MRT_NODE_QUORUM;
+#ifndef MRT_CAMERA_QUORUM
+#define MRT_CAMERA_QUORUM 16
+#endif
+constexpr int kCameraQuorum = MRT_CAMERA_QUORUM;   // for a pass of camera rays
 template <int Q = kNodeQuorum>
 __device__ __forceinline__ bool node_phase_over(bool searching, bool holding_leaf) {
     const uint32_t s = __ballot_sync(0xFFFFFFFFu, searching);
@@ -57,7 +62,13 @@ __device__ __forceinline__ void start_ray(const DevScene &s, const Ray &r, FastT
     trav_begin<kCount>(s, r, len, id, t);   // the plane or sphere hit stays the answer unless a triangle is closer
 }
 
-template <bool kCount, class Work, class Lane, class Stack, int Q = kNodeQuorum>
+// idle lanes of a warp that trigger a refill (all idle lanes refill then, with one atomic)
+#ifndef MRT_REFILL_MIN
+#define MRT_REFILL_MIN 8
+#endif
+constexpr int kRefillMin = MRT_REFILL_MIN;
+
+template <bool kCount, class Work, class Lane, class Stack, int Q = kNodeQuorum, int R = kRefillMin>
 __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, Stack &stk) {
     const uint32_t FULL = 0xFFFFFFFFu;
     const int lane_id = threadIdx.x & 31;
@@ -69,7 +80,7 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, St
     for (;;) {
         // 1. refill idle lanes (one atomic per warp)
         const uint32_t idle = __ballot_sync(FULL, !active);
-        if (!exhausted && (__popc(idle) >= 8 || idle == FULL)) {
+        if (!exhausted && (__popc(idle) >= R || idle == FULL)) {
             const int leader = __ffs(idle) - 1;
             uint32_t base = 0;
             if (lane_id == leader) base = atomicAdd(work.counter(), (uint32_t)__popc(idle));
@@ -108,10 +119,10 @@ __device__ void persistent_closest(const DevScene &s, Work &work, Lane &lane, St
 }
 
 // the same with the stack in local memory
-template <bool kCount, int Q = kNodeQuorum, class Work, class Lane>
+template <bool kCount, int Q = kNodeQuorum, int R = kRefillMin, class Work, class Lane>
 __device__ __forceinline__ void persistent_closest(const DevScene &s, Work &work, Lane &lane) {
     TravStack stk;
-    persistent_closest<kCount, Work, Lane, TravStack, Q>(s, work, lane, stk);
+    persistent_closest<kCount, Work, Lane, TravStack, Q, R>(s, work, lane, stk);
 }
 
 }  // namespace mrt

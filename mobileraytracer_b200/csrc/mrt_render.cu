@@ -209,10 +209,12 @@ struct NsTraceWork {
 #endif
 constexpr bool kNsSplit = MRT_NS_SPLIT != 0;
 // node-phase quorum of the NoShadows traversal (coherent camera rays)
-#ifndef MRT_NS_QUORUM
-#define MRT_NS_QUORUM 8
+constexpr int kNsQuorum = kCameraQuorum;
+// idle lanes that trigger a refill in the NoShadows traversal
+#ifndef MRT_NS_REFILL
+#define MRT_NS_REFILL 8
 #endif
-constexpr int kNsQuorum = MRT_NS_QUORUM;
+constexpr int kNsRefill = MRT_NS_REFILL;
 constexpr uint32_t kNsChunk = 1u << 22;
 
 __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, NsTraceWork w, RenderParams p) {
@@ -222,9 +224,9 @@ __global__ void __launch_bounds__(128, kNsBlocksPerSm) k_ns_trace(DevScene s, Ns
         __shared__ uint2 stack_cols[(kNsSmemStack > 0 ? kNsSmemStack : 1) * 128];
         SharedTravStack<(kNsSmemStack > 0 ? kNsSmemStack : 1), 128> stk;
         stk.col = stack_cols + threadIdx.x;
-        persistent_closest<false, NsTraceWork, NsTraceLane, decltype(stk), kNsQuorum>(s, w, lane, stk);
+        persistent_closest<false, NsTraceWork, NsTraceLane, decltype(stk), kNsQuorum, kNsRefill>(s, w, lane, stk);
     } else {
-        persistent_closest<false, kNsQuorum>(s, w, lane);
+        persistent_closest<false, kNsQuorum, kNsRefill>(s, w, lane);
     }
 }
 
@@ -484,11 +486,13 @@ struct ShadowWork {
 #endif
 constexpr int kWaveBlocksPerSm = MRT_WAVE_BLOCKS_PER_SM;
 
+// Q: node-phase quorum (the camera rays of level 0 are coherent, the bounces are not)
+template <int Q>
 __global__ void __launch_bounds__(128, kWaveBlocksPerSm) k_wave_extend_fast(DevScene s, WaveState w, int level, uint32_t *ctr) {
     const Level L = clamp_level(w, w.levels[level]);
     ExtendWork work{w, L, ctr};
     WaveLane lane;
-    persistent_closest<false>(s, work, lane);
+    persistent_closest<false, Q>(s, work, lane);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[0], (unsigned long long)L.count);
 }
 
@@ -694,7 +698,8 @@ void launch_wave_level(const DevScene &s, const RenderParams &p, const WaveState
                        uint32_t *ctrs) {
     if (ACCEL == MRT_ACCEL_BVH && MODE == MRT_BVH_FAST) {
         // counters [2 * level] and [2 * level + 1] were zeroed for this wave
-        k_wave_extend_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
+        if (level == 0) k_wave_extend_fast<kCameraQuorum><<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
+        else k_wave_extend_fast<kNodeQuorum><<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level);
         if (w.sort_shading) k_wave_shade_sorted<<<grid, 128, 0, q>>>(s, p, w, level);
         else k_wave_shade<<<grid, 128, 0, q>>>(s, p, w, level);
         k_wave_shadow_fast<<<grid, 128, 0, q>>>(s, w, level, ctrs + 2 * level + 1);
