@@ -474,8 +474,7 @@ BatchState state_of(MrtBatch *b, int pipe) {
 
 template <int kBlock>
 void launch_traversal(const BatchState &s, int level, int grid, cudaStream_t q, bool extend) {
-    if (extend && level == 0) k_batch_extend<kBlock, kCameraQuorum><<<grid, kBlock, 0, q>>>(s, level);   // camera rays
-    else if (extend) k_batch_extend<kBlock, kNodeQuorum><<<grid, kBlock, 0, q>>>(s, level);
+    if (extend) k_batch_extend<kBlock, kNodeQuorum><<<grid, kBlock, 0, q>>>(s, level);
     else k_batch_shadow<kBlock><<<grid, kBlock, 0, q>>>(s, level);
 }
 

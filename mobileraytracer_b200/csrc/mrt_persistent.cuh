@@ -33,7 +33,7 @@ constexpr int kNodeQuorum = MRT_NODE_QUORUM;
 #ifndef MRT_CAMERA_QUORUM
 #define MRT_CAMERA_QUORUM 16
 #endif
-constexpr int kCameraQuorum = MRT_CAMERA_QUORUM;   // for a pass of camera rays
+constexpr int kCameraQuorum = MRT_CAMERA_QUORUM;   // for a pass of camera rays (the NoShadows trace)
 template <int Q = kNodeQuorum>
 __device__ __forceinline__ bool node_phase_over(bool searching, bool holding_leaf) {
     const uint32_t s = __ballot_sync(0xFFFFFFFFu, searching);
