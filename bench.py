@@ -434,6 +434,9 @@ def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, g
     kernel_ms = trace_ms if trace_ms > 0 else ms
     achieved = alg / (kernel_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "note": ("algorithmic bytes are the node, triangle and hit records the traversal fetches; the scene "
+                     "stays in L2, so they are served by L1/L2 and frac can exceed 1; dram_frac (from the ncu "
+                     "capture of this source) is the DRAM use"),
             "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
             "bytes_per_ray": alg / len(rays_np), **counts, "kernel": kernel}
     if profile:

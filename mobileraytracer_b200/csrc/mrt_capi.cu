@@ -221,6 +221,9 @@ int mrt_context_create(int device, MrtContext **out) {
         if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&e), "event");
     for (int k = 0; k < 2 && st == MRT_OK; ++k)
         st = cuda_status(ctx, cudaEventCreateWithFlags(&ctx->wave_ev[k], cudaEventDisableTiming), "event");
+    for (int k = 0; k < MrtContext::kHostBands && st == MRT_OK; ++k)
+        st = cuda_status(ctx, cudaEventCreateWithFlags(&ctx->band_ev[k], cudaEventDisableTiming), "event");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "stream");
     if (st != MRT_OK) {
         fprintf(stderr, "mrt_context_create: %s\n", ctx->error.c_str());
         mrt_context_destroy(ctx);
@@ -234,6 +237,7 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto &b : ctx->scratch) dev_free(b);
     for (auto &b : ctx->wave) dev_free(b);
     for (auto &b : ctx->raster) dev_free(b);
@@ -243,6 +247,8 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (auto &e : ctx->trace_ev) if (e) cudaEventDestroy(e);
     for (auto &e : ctx->wave_ev) if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->band_ev) if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -312,6 +318,7 @@ static void scene_free(MrtScene *s) {
                       &s->pln_n, &s->pln_p, &s->pln_mat, &s->lights, &s->mats, &s->fnodes, &s->ftris};
     for (DevBuf *b : bufs) dev_free(*b);
     for (int k = 0; k < 3; ++k) { dev_free(s->rnodes[k]); dev_free(s->grid_start[k]); dev_free(s->grid_refs[k]); }
+    dev_free(s->grid_trec);
     for (auto &b : s->work) dev_free(b);
 }
 
@@ -486,6 +493,8 @@ int mrt_scene_build(MrtScene *s, const MrtAccelOpts *o) {
     dev_free(s->fnodes);
     dev_free(s->ftris);
     for (int k = 0; k < 3; ++k) { dev_free(s->rnodes[k]); dev_free(s->grid_start[k]); dev_free(s->grid_refs[k]); }
+    dev_free(s->grid_trec);
+    s->dev.grid[kTriangle].trec = nullptr;
     s->dev.accel = o->accelerator;
     s->dev.bvh_mode = o->bvh_mode;
     int st = MRT_OK;
@@ -509,6 +518,7 @@ uint64_t mrt_scene_device_bytes(const MrtScene *s) {
                             &s->pln_n, &s->pln_p, &s->pln_mat, &s->lights, &s->mats, &s->fnodes, &s->ftris};
     for (const DevBuf *b : bufs) t += b->bytes;
     for (int k = 0; k < 3; ++k) t += s->rnodes[k].bytes + s->grid_start[k].bytes + s->grid_refs[k].bytes;
+    t += s->grid_trec.bytes;
     return t;
 }
 

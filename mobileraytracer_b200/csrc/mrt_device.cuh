@@ -123,6 +123,8 @@ struct DevGrid {
     V3 sr, cw;          // m_SR, m_CW
     const uint32_t *start;  // G^3 + 1
     const uint32_t *refs;
+    const float *trec;      // triangle grid: 16 floats per triangle in input order (A, AB, AC, 7 unused),
+                            // 64-byte aligned records the walk reads with one 256-bit and one 32-bit load
 };
 
 enum PrimType { kPlane = 0, kSphere = 1, kTriangle = 2 };

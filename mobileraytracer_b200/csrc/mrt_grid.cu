@@ -239,6 +239,23 @@ void launch_fill(MrtScene *s, const GridBuildParams &p, uint32_t n, uint32_t *co
 
 }  // namespace
 
+// the triangle grid's packed records: A, AB, AC in 9 of 16 floats (one 64-byte record per triangle)
+#ifndef MRT_GRID_TRIREC
+#define MRT_GRID_TRIREC 1
+#endif
+constexpr bool kGridTriRecords = MRT_GRID_TRIREC != 0;
+__global__ void k_pack_trec(uint32_t n, const float4 *__restrict__ a, const float4 *__restrict__ ab,
+                            const float4 *__restrict__ ac, float *out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 A = a[i], B = ab[i], C = ac[i];
+    float4 *r = reinterpret_cast<float4 *>(out + 16 * (size_t)i);
+    r[0] = make_float4(A.x, A.y, A.z, B.x);
+    r[1] = make_float4(B.y, B.z, C.x, C.y);
+    r[2] = make_float4(C.z, 0.0f, 0.0f, 0.0f);
+    r[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 namespace mrt_host {
 
 int build_grids(MrtScene *s, const float *cam_min, const float *cam_max, int grid_size, int grid_index) {
@@ -321,6 +338,15 @@ int build_grids(MrtScene *s, const float *cam_min, const float *cam_max, int gri
         if (st != MRT_OK) return st;
         g.start = (const uint32_t *)s->grid_start[type].ptr;
         g.refs = (const uint32_t *)s->grid_refs[type].ptr;
+        g.trec = nullptr;
+        if (type == kTriangle && n > 0 && kGridTriRecords) {
+            st = dev_alloc(ctx, s->grid_trec, 64ull * n);
+            if (st != MRT_OK) return st;
+            k_pack_trec<<<(n + 255) / 256, 256, 0, q>>>(n, s->dev.tri_a, s->dev.tri_ab, s->dev.tri_ac, (float *)s->grid_trec.ptr);
+            st = cuda_status(ctx, cudaGetLastError(), "grid records");
+            if (st != MRT_OK) return st;
+            g.trec = (const float *)s->grid_trec.ptr;
+        }
     }
     return MRT_OK;
 }

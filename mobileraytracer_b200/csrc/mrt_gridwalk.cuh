@@ -37,15 +37,41 @@ struct GridWalk {
     uint32_t id;
     uint32_t steps;
     uint32_t b, k, e;   // the current cell's references: first, next to test, end
+    uint32_t ref;       // refs[k], loaded one test ahead
     uint8_t phase;      // 1: first walk, 2: testloop, 0: finished
     bool tri_hit;       // a triangle of the grid accepted (ends the first walk)
 };
+
+__device__ __forceinline__ uint32_t grid_ref(const DevGrid &g, uint32_t k, uint32_t e) { return k < e ? __ldg(&g.refs[k]) : 0u; }
 
 __device__ __forceinline__ void grid_walk_load(const DevGrid &g, GridWalk &w) {
     const uint32_t c = grid_cell(g, w.st.X, w.st.Y, w.st.Z);
     w.b = __ldg(&g.start[c]);
     w.e = __ldg(&g.start[c + 1]);
     w.k = w.b;
+    w.ref = grid_ref(g, w.k, w.e);
+}
+
+// triangle i of the grid with the reference accept rule (triangle_hit), its edges from the grid's
+// packed record when the build made them
+__device__ __forceinline__ bool grid_tri_hit(const DevScene &s, const DevGrid &g, uint32_t i, const Ray &r, float &len,
+                                             uint32_t &id) {
+    if (!g.trec) return triangle_hit(s, i, r, len, id);
+    const uint32_t self = hid(MRT_PRIM_TRIANGLE, i);
+    if (r.exclude == self) return false;
+    const float *rec = g.trec + 16 * (size_t)i;
+    uint4 p0, p1;
+    ldg_32b(reinterpret_cast<const uint4 *>(rec), p0, p1);
+    const float acz = __ldg(rec + 8);
+    const V3 a{__uint_as_float(p0.x), __uint_as_float(p0.y), __uint_as_float(p0.z)};
+    const V3 ab{__uint_as_float(p0.w), __uint_as_float(p1.x), __uint_as_float(p1.y)};
+    const V3 ac{__uint_as_float(p1.z), __uint_as_float(p1.w), acz};
+    float t, u, v;
+    if (!tri_test(a, ab, ac, r, t, u, v)) return false;
+    if (t >= len) return false;
+    len = t;
+    id = self;
+    return true;
 }
 
 // planes and spheres walk their own grids first (Shader.cpp:124-150), whole, in this lane
@@ -93,12 +119,15 @@ __device__ __forceinline__ bool grid_testloop_step(GridWalk &w) {
 __device__ __forceinline__ void grid_walk_step(const DevScene &s, const Ray &r, GridWalk &w) {
     const DevGrid &g = s.grid[kTriangle];
     if (w.k < w.e) {
-        const bool h = triangle_hit(s, __ldg(&g.refs[w.k]), r, w.len, w.id);
+        const uint32_t i = w.ref;
         ++w.k;
+        w.ref = grid_ref(g, w.k, w.e);   // the next reference's index, while this one is tested
+        const bool h = grid_tri_hit(s, g, i, r, w.len, w.id);
         if (w.phase == 1 && h) {   // the first walk ends; the testloop starts over this same cell
             w.tri_hit = true;
             w.phase = 2;
             w.k = w.b;
+            w.ref = grid_ref(g, w.k, w.e);
         }
         return;
     }

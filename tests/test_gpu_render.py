@@ -152,6 +152,35 @@ def test_host_path_keeps_unrendered_rows(ctx):
     g.close()
 
 
+def test_host_path_row_bands_equal_the_device_path(ctx):
+    """Host buffers on the NoShadows trace + shade path: the frame renders in row bands whose rows are
+    copied out while the next band renders.  Bitmap and sums equal the device path for several bands,
+    an odd width (row-major tasks), the RegularGrid, several samples per pixel and a padded row pitch
+    (which takes the single copy at the end)."""
+    torch = pytest.importorskip("torch")
+    soup = scenes.triangle_soup(20_000, 5, 320, 240)
+    for accel, w, h, spp in ((capi.MRT_ACCEL_BVH, 320, 240, 1), (capi.MRT_ACCEL_BVH, 97, 200, 3),
+                             (capi.MRT_ACCEL_REGULAR_GRID, 320, 240, 2)):
+        g = Scene(ctx, soup).build(accel)
+        opts = capi.render_opts(shader=NS, width=w, height=h, spp=spp, spl=1, seed=9)
+        host_bm = np.full((h, w), 0x12345678, np.uint32)
+        host_acc = np.zeros((h, w, 4), np.float32)
+        _, _, st = g.render(soup.camera, opts, bitmap=host_bm, accum=host_acc)
+        assert st.kernel_launches == 8   # four bands of whole 16-row stripes, a trace and a shade each
+        dev_bm = torch.full((h * w,), 0x12345678, dtype=torch.int32, device="cuda")
+        dev_acc = torch.zeros(h * w * 4, dtype=torch.float32, device="cuda")
+        g.render(soup.camera, opts, bitmap=dev_bm, accum=dev_acc)
+        torch.cuda.synchronize()
+        assert np.array_equal(host_bm, dev_bm.cpu().numpy().view(np.uint32).reshape(h, w)), (accel, w, h)
+        assert np.array_equal(host_acc.view(np.uint32), dev_acc.cpu().numpy().view(np.uint32).reshape(h, w, 4))
+        # a padded row pitch: one copy at the end, same pixels
+        pitch = w + 3
+        padded = np.full((h, pitch), 0x12345678, np.uint32)
+        g.render(soup.camera, opts, bitmap=padded, stride_bytes=4 * pitch)
+        assert np.array_equal(padded[:, :w], host_bm) and (padded[:, w:] == 0x12345678).all()
+        g.close()
+
+
 def test_errors_are_reported(ctx):
     import mobileraytracer_b200 as m
     sc = scenes.glass_room()
