@@ -46,9 +46,6 @@ struct MrtContext {
     static constexpr int kTraceEvents = 16;             // start / end pairs around traversal launches
     cudaEvent_t trace_ev[2 * kTraceEvents] = {};
     cudaEvent_t wave_ev[2] = {nullptr, nullptr};   // the last two waves of a render (bounded run-ahead)
-    static constexpr int kHostBands = 4;            // row bands a host-memory render copies out as it goes
-    cudaStream_t copy_stream = nullptr;
-    cudaEvent_t band_ev[kHostBands] = {};
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];
     MrtArena *arena = nullptr;          // device allocations of this context come from here when set
@@ -112,16 +109,8 @@ int build_grids(MrtScene *s, const float *camera_min, const float *camera_max, i
 int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits);
 int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uint32_t n, uint8_t *d_occ);
 int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris);
-// Host buffers a render copies its finished row bands into while it goes on (mrt_render with host
-// memory): set by the caller, `rows_done` set by the render when every rendered row has been queued
-// on the context's copy stream (the caller then waits for that stream instead of copying the bitmap).
-struct HostOut {
-    uint32_t *bitmap = nullptr;   // host bitmap, row pitch 4 * width
-    float *accum = nullptr;       // host sums or nullptr
-    bool rows_done = false;
-};
 int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-           float *d_accum, MrtRenderStats *stats, HostOut *out = nullptr);
+           float *d_accum, MrtRenderStats *stats);
 
 mrt::DevCamera make_camera(const MrtCamera &c);
 void camera_box(const MrtCamera &c, float *mn, float *mx);

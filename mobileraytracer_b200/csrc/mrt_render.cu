@@ -208,11 +208,6 @@ struct NsTraceWork {
 #define MRT_NS_SPLIT 1
 #endif
 constexpr bool kNsSplit = MRT_NS_SPLIT != 0;
-// host-memory renders copy finished row bands out while the rest renders (0: one copy at the end)
-#ifndef MRT_HOST_BANDS
-#define MRT_HOST_BANDS 1
-#endif
-constexpr bool kHostBandsOn = MRT_HOST_BANDS != 0;
 // node-phase quorum of the NoShadows traversal (coherent camera rays)
 constexpr int kNsQuorum = kCameraQuorum;
 // idle lanes that trigger a refill in the NoShadows traversal
@@ -759,7 +754,7 @@ uint32_t wave_roots_setting() {
 namespace mrt_host {
 
 static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-                       float *d_accum, MrtRenderStats *stats, uint32_t strata, HostOut *out = nullptr) {
+                       float *d_accum, MrtRenderStats *stats, uint32_t strata) {
     MrtContext *ctx = s->ctx;
     cudaStream_t q = ctx->stream;
     const uint32_t stride_px = stride / 4u;
@@ -841,19 +836,11 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             if (s->stop.load()) return cancelled(ctx, q);
             if ((fast || accel == MRT_ACCEL_REGULAR_GRID) && kNsSplit) {
                 // chunks of at most kNsChunk (sample, pixel) items: whole samples of up to kNsChunk pixels.
-                // With host buffers to fill (a single implicit round on the plain rectangle), the pixels
-                // go in up to kHostBands bands of whole 16-row stripes, and each band's rows are copied
-                // to the host on the copy stream while the next band renders.
+                // (Rendering a host-memory frame in four row bands, each copied out while the next band
+                // rendered, was slower end to end on the 1080p soup frame: 1121 against 1496 Mrays/s —
+                // each shorter traversal launch pays its own tail.)
                 const uint32_t count = plan.round_count[r];
-                uint32_t n_pix_max = std::min<uint32_t>(count, kNsChunk);
-                const uint32_t stripe = 16u * o->width;
-                const bool banded = out && out->bitmap && plan.implicit && plan.round_first.size() == 1 &&
-                                    stride == 4u * o->width && count % stripe == 0 && count / stripe >= 2;
-                if (banded) {
-                    const uint32_t stripes = count / stripe;
-                    const uint32_t per_band = (stripes + MrtContext::kHostBands - 1) / MrtContext::kHostBands;
-                    n_pix_max = std::min<uint32_t>(per_band * stripe, (kNsChunk / stripe) * stripe);
-                }
+                const uint32_t n_pix_max = std::min<uint32_t>(count, kNsChunk);
                 st = ensure(ctx, ctx->wave[1], sizeof(uint2) * (size_t)kNsChunk);
                 if (st != MRT_OK) return st;
                 uint2 *hits = (uint2 *)ctx->wave[1].ptr;
@@ -875,18 +862,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                         k_ns_shade<<<(n_pix + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0, n_pix, s0, n_s,
                                                                         tiles_x, hits);
                     }
-                    if (banded) {   // the band's rows are final: to the host while the next band renders
-                        const int slot = (int)((j0 / n_pix_max) % MrtContext::kHostBands);
-                        const size_t px0 = j0, npx = n_pix;   // whole rows: j0 and n_pix are multiples of the width
-                        cudaEventRecord(ctx->band_ev[slot], q);
-                        cudaStreamWaitEvent(ctx->copy_stream, ctx->band_ev[slot], 0);
-                        cudaMemcpyAsync(out->bitmap + px0, d_bitmap + px0, 4 * npx, cudaMemcpyDeviceToHost, ctx->copy_stream);
-                        if (out->accum && d_accum)
-                            cudaMemcpyAsync(out->accum + 4 * px0, d_accum + 4 * px0, 16 * npx, cudaMemcpyDeviceToHost,
-                                            ctx->copy_stream);
-                    }
                 }
-                if (banded) out->rows_done = true;
             } else if (fast) {
                 cudaMemsetAsync(ctx->d_counters, 0, sizeof(uint32_t), q);
                 k_render_noshadows_fast<<<ctx->sm_count * kNsBlocksPerSm, 128, 0, q>>>(s->dev, p, plan.round_first[r],
@@ -1005,8 +981,8 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
 }
 
 int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-           float *d_accum, MrtRenderStats *stats, HostOut *out) {
-    return render_impl(s, cam, o, d_bitmap, stride, d_accum, stats, o->spp, out);
+           float *d_accum, MrtRenderStats *stats) {
+    return render_impl(s, cam, o, d_bitmap, stride, d_accum, stats, o->spp);
 }
 
 }  // namespace mrt_host
@@ -1061,17 +1037,8 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
             st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");
         if (st != MRT_OK) return st;
     }
-    HostOut out;
-    if (mem == MRT_MEM_HOST && kHostBandsOn) {
-        out.bitmap = bitmap;
-        out.accum = accum;
-    }
-    st = render(s, cam, o, d_bitmap, stride_bytes, d_accum, stats, mem == MRT_MEM_HOST ? &out : nullptr);
-    if (mem == MRT_MEM_HOST && out.rows_done) {
-        // every rendered row is on its way (the rows below the block schedule were never changed)
-        const int cs = cuda_status(ctx, cudaStreamSynchronize(ctx->copy_stream), "render copy out");
-        if (st == MRT_OK) st = cs;
-    } else if (st == MRT_OK && mem == MRT_MEM_HOST) {
+    st = render(s, cam, o, d_bitmap, stride_bytes, d_accum, stats);
+    if (st == MRT_OK && mem == MRT_MEM_HOST) {
         st = cuda_status(ctx, cudaMemcpyAsync(bitmap, d_bitmap, bm_bytes, cudaMemcpyDeviceToHost, ctx->stream), "bitmap out");
         if (st == MRT_OK && accum)
             st = cuda_status(ctx, cudaMemcpyAsync(accum, d_accum, acc_bytes, cudaMemcpyDeviceToHost, ctx->stream), "accum out");

@@ -152,11 +152,10 @@ def test_host_path_keeps_unrendered_rows(ctx):
     g.close()
 
 
-def test_host_path_row_bands_equal_the_device_path(ctx):
-    """Host buffers on the NoShadows trace + shade path: the frame renders in row bands whose rows are
-    copied out while the next band renders.  Bitmap and sums equal the device path for several bands,
-    an odd width (row-major tasks), the RegularGrid, several samples per pixel and a padded row pitch
-    (which takes the single copy at the end)."""
+def test_host_path_trace_and_shade_equal_the_device_path(ctx):
+    """Host buffers on the NoShadows trace + shade path: bitmap and sums equal the device path on the
+    FAST BVH and the RegularGrid, for an odd width (row-major tasks), several samples per pixel, and with
+    a padded row pitch."""
     torch = pytest.importorskip("torch")
     soup = scenes.triangle_soup(20_000, 5, 320, 240)
     for accel, w, h, spp in ((capi.MRT_ACCEL_BVH, 320, 240, 1), (capi.MRT_ACCEL_BVH, 97, 200, 3),
@@ -166,18 +165,22 @@ def test_host_path_row_bands_equal_the_device_path(ctx):
         host_bm = np.full((h, w), 0x12345678, np.uint32)
         host_acc = np.zeros((h, w, 4), np.float32)
         _, _, st = g.render(soup.camera, opts, bitmap=host_bm, accum=host_acc)
-        assert st.kernel_launches == 8   # four bands of whole 16-row stripes, a trace and a shade each
+        assert st.kernel_launches >= 2 and st.kernel_launches % 2 == 0   # trace and shade passes
         dev_bm = torch.full((h * w,), 0x12345678, dtype=torch.int32, device="cuda")
         dev_acc = torch.zeros(h * w * 4, dtype=torch.float32, device="cuda")
         g.render(soup.camera, opts, bitmap=dev_bm, accum=dev_acc)
         torch.cuda.synchronize()
         assert np.array_equal(host_bm, dev_bm.cpu().numpy().view(np.uint32).reshape(h, w)), (accel, w, h)
         assert np.array_equal(host_acc.view(np.uint32), dev_acc.cpu().numpy().view(np.uint32).reshape(h, w, 4))
-        # a padded row pitch: one copy at the end, same pixels
+        # a padded row pitch (the block schedule then depends on the pitch, Renderer.cpp:82-93): one copy
+        # at the end, the same bitmap as the device path with that pitch
         pitch = w + 3
         padded = np.full((h, pitch), 0x12345678, np.uint32)
         g.render(soup.camera, opts, bitmap=padded, stride_bytes=4 * pitch)
-        assert np.array_equal(padded[:, :w], host_bm) and (padded[:, w:] == 0x12345678).all()
+        dev_pad = torch.full((h * pitch,), 0x12345678, dtype=torch.int32, device="cuda")
+        g.render(soup.camera, opts, bitmap=dev_pad, stride_bytes=4 * pitch)
+        torch.cuda.synchronize()
+        assert np.array_equal(padded, dev_pad.cpu().numpy().view(np.uint32).reshape(h, pitch))
         g.close()
 
 
