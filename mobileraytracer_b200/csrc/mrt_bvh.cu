@@ -332,9 +332,17 @@ __device__ __forceinline__ float half_area(float4 lo, float4 hi) {
 // kTriCost per triangle; an inner node costs kNodeCost plus its two children's costs, each weighted
 // by the share of the node's box area its box has.  The unit is one box test: 2.2 box tests per
 // triangle test and 2 per opened inner node fit the frame times of the 1,000,000-triangle soup at
-// leaves of 1, 2 and 3 triangles.  Scattered small triangles (the soups) end up one per leaf: two
+// leaves of 1, 2 and 3 triangles, and still do for the 8-wide tree (node cost 1 or triangle cost 4:
+// equal; node cost 4: -11 % on the soup frame, triangle cost 1.2: -6 %; the terrain PathTracer within
+// 0.2 % except node cost 4 and triangle cost 1.2, -3 %).  Scattered small triangles (the soups) end up one per leaf: two
 // boxes cull better than two triangle tests; touching triangles (a heightfield) stay in pairs.
-constexpr float kTriCost = 2.2f, kNodeCost = 2.0f;
+#ifndef MRT_BVH_TRI_COST
+#define MRT_BVH_TRI_COST 2.2f
+#endif
+#ifndef MRT_BVH_NODE_COST
+#define MRT_BVH_NODE_COST 2.0f
+#endif
+constexpr float kTriCost = MRT_BVH_TRI_COST, kNodeCost = MRT_BVH_NODE_COST;
 constexpr int kLeafCostDepth = 3;   // inner levels of a subtree of up to 4 triangles
 
 struct BinView {
