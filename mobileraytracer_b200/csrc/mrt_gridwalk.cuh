@@ -18,12 +18,6 @@
 
 namespace mrt {
 
-// One reference test or one cell step per call (MRT_GRID_CURSOR, the default), so the lanes of a warp
-// do the same small piece of work each iteration; 0: one whole cell per call.  On the 1080p soup frame
-// at G = 128 (trace and shade kernels, 7 blocks per SM): 285 Mrays/s against 207 a cell at a time.
-#ifndef MRT_GRID_CURSOR
-#define MRT_GRID_CURSOR 1
-#endif
 // resident blocks of 128 threads per SM for the kernels of the persistent grid walk (7: 72 registers,
 // no spills; 285 Mrays/s on that frame against 270 at 8 and 247 at 6)
 #ifndef MRT_GRID_BLOCKS_PER_SM
@@ -31,6 +25,9 @@ namespace mrt {
 #endif
 constexpr int kGridBlocksPerSm = MRT_GRID_BLOCKS_PER_SM;
 
+// A lane's walk advances by one reference test or one cell step per iteration, so the lanes of a warp do
+// the same small piece of work each iteration (a whole cell per iteration: 207 against 285 Mrays/s on the
+// 1080p soup frame at G = 128, before the packed triangle records).
 struct GridWalk {
     Dda st;
     float len;
@@ -110,7 +107,6 @@ __device__ __forceinline__ bool grid_testloop_step(GridWalk &w) {
     return !out;
 }
 
-#if MRT_GRID_CURSOR
 // one reference of the current cell, or the move to the next cell (RegularGrid.hpp:236-335)
 __device__ __forceinline__ void grid_walk_step(const DevScene &s, const Ray &r, GridWalk &w) {
     const DevGrid &g = s.grid[kTriangle];
@@ -130,26 +126,6 @@ __device__ __forceinline__ void grid_walk_step(const DevScene &s, const Ray &r, 
     if (++w.steps > kMaxGridSteps) { raise_error(s, MRT_ERR_LIMIT); w.phase = 0; return; }
     grid_walk_load(g, w);
 }
-#else
-// one cell of the lane's walk (RegularGrid.hpp:236-335)
-__device__ __forceinline__ void grid_walk_step(const DevScene &s, const Ray &r, GridWalk &w) {
-    const DevGrid &g = s.grid[kTriangle];
-    const uint32_t c = grid_cell(g, w.st.X, w.st.Y, w.st.Z);
-    const uint32_t b = __ldg(&g.start[c]), e = __ldg(&g.start[c + 1]);
-    if (w.phase == 1) {
-        for (uint32_t k = b; k < e; ++k) {
-            w.tri_hit |= triangle_hit(s, __ldg(&g.refs[k]), r, w.len, w.id);
-            if (w.tri_hit) { w.phase = 2; return; }   // testloop starts over this same cell
-        }
-        if (!dda_step(w.st)) { w.phase = 0; return; }
-        if (++w.steps > kMaxGridSteps) { raise_error(s, MRT_ERR_LIMIT); w.phase = 0; }
-        return;
-    }
-    for (uint32_t k = b; k < e; ++k) triangle_hit(s, __ldg(&g.refs[k]), r, w.len, w.id);
-    if (!grid_testloop_step(w)) { w.phase = 0; return; }
-    if (++w.steps > kMaxGridSteps) { raise_error(s, MRT_ERR_LIMIT); w.phase = 0; }
-}
-#endif
 
 // Work provides total(), counter(), begin(item, lane, r) and
 // finish(lane, r, hit, t, id, const FastTrav &) -> true: r holds the item's next ray (as persistent_closest)

@@ -580,21 +580,6 @@ struct TravStack {
     __device__ __forceinline__ uint2 get(int i) const { return e[i]; }
 };
 
-// the first K entries in this thread's column of a block-wide shared array (entry i at col[i * B],
-// B = threads per block), the rest in local memory.  Lanes whose stacks have different depths still
-// touch distinct banks (a column per thread), where their local-memory entries would fall into
-// distinct sectors.
-template <int K, int B>
-struct SharedTravStack {
-    uint2 *col;
-    uint2 e[kFastStack - K];
-    __device__ __forceinline__ void put(int i, uint2 v) {
-        if (i < K) col[i * B] = v;
-        else e[i - K] = v;
-    }
-    __device__ __forceinline__ uint2 get(int i) const { return i < K ? col[i * B] : e[i - K]; }
-};
-
 template <bool kCount, class S>
 __device__ __forceinline__ void trav_begin(const S &s, const Ray &r, float len0, uint32_t id0, FastTrav &t) {
     t.f = fast_ray(r);
