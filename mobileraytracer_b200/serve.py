@@ -317,6 +317,7 @@ class _DeviceBackend:
         import torch
         self.torch = torch
         self.ctx = ctx
+        self.device = f"cuda:{device}"
         self.builder = _Builder(device, arena, ctx, pool_scene)
         self.scenes: dict[int, object] = {}
         self.bitmaps: dict[int, object] = {}
@@ -344,7 +345,7 @@ class _DeviceBackend:
     def bitmap(self, r: Request):
         bm = self.bitmaps.get(r.scene)
         if bm is None:
-            bm = self.torch.zeros(r.side * r.side, dtype=self.torch.int32, device="cuda")
+            bm = self.torch.zeros(r.side * r.side, dtype=self.torch.int32, device=self.device)
             self.bitmaps[r.scene] = bm
         return bm
 
