@@ -382,11 +382,12 @@ def time_e2e(scene, sc, opts, n: int, accum: bool = False):
     for _ in range(n):
         scene.render(sc.camera, opts, bitmap=host_bm, accum=host_acc)
     e2e_s = (time.perf_counter() - t) / n
-    acc_bytes = host_acc.nbytes if accum else 0
-    # in: the rows the block schedule leaves alone (a first pass overwrites the rest without reading
-    # them), the camera and the options; out: the whole bitmap (and sums)
-    h2d = host_bm.nbytes - 4 * w * 16 * (h // 16) + acc_bytes + 64 + 100
-    return e2e_s, h2d, host_bm.nbytes + acc_bytes
+    # the block schedule of these frames is the plain rectangle of rows 0 .. 16 * (h // 16) - 1, and
+    # only those rows travel: in, the sums (a first pass overwrites the bitmap rows without reading
+    # them), the camera and the options; out, the bitmap rows (and sums)
+    rows_px = w * 16 * (h // 16)
+    acc_bytes = 16 * rows_px if accum else 0
+    return e2e_s, acc_bytes + 64 + 100, 4 * rows_px + acc_bytes
 
 
 def soup_frame(dist, ctx, sc, args, accel: int, mode: int, grid_size: int = 0, grid_index: int = 0,

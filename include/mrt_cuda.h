@@ -296,7 +296,10 @@ int mrt_trace_closest_counts(MrtScene *scene, const MrtRay *rays, uint32_t n, ui
 /* One Renderer::renderFrame: for sample = spp_offset .. spp_offset+spp-1 every pixel the reference's
  * 16x16 block schedule covers gets bitmap = incrementalAvg(rgb, bitmap, sample + 1); other pixels
  * are left untouched.  stride_bytes / 4 is the row pitch in pixels.  accum (optional, 4 floats per
- * pixel at width*height) receives the per-pixel sum of the fp32 sample values, in sample order. */
+ * pixel at width*height) receives the per-pixel sum of the fp32 sample values, in sample order.
+ * With MRT_MEM_HOST the call returns once the result is in the caller's buffers; on the plain
+ * rectangle (row pitch 4 * width) only the scheduled rows are copied, and page-locked buffers
+ * (cudaHostAlloc / cudaHostRegister) let it copy finished rows out while it shades the rest. */
 int mrt_render(MrtScene *scene, const MrtCamera *camera, const MrtRenderOpts *opts,
                uint32_t *bitmap, uint32_t stride_bytes, float *accum, uint32_t mem,
                MrtRenderStats *stats);

@@ -221,6 +221,9 @@ int mrt_context_create(int device, MrtContext **out) {
         if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreate(&e), "event");
     for (int k = 0; k < 2 && st == MRT_OK; ++k)
         st = cuda_status(ctx, cudaEventCreateWithFlags(&ctx->wave_ev[k], cudaEventDisableTiming), "event");
+    for (auto &e : ctx->band_ev)
+        if (st == MRT_OK) st = cuda_status(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    if (st == MRT_OK) st = cuda_status(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "stream");
 
     if (st != MRT_OK) {
         fprintf(stderr, "mrt_context_create: %s\n", ctx->error.c_str());
@@ -235,6 +238,7 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto &b : ctx->scratch) dev_free(b);
     for (auto &b : ctx->wave) dev_free(b);
     for (auto &b : ctx->raster) dev_free(b);
@@ -244,6 +248,8 @@ void mrt_context_destroy(MrtContext *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (auto &e : ctx->trace_ev) if (e) cudaEventDestroy(e);
     for (auto &e : ctx->wave_ev) if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->band_ev) if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

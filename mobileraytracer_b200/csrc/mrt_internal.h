@@ -46,6 +46,9 @@ struct MrtContext {
     static constexpr int kTraceEvents = 16;             // start / end pairs around traversal launches
     cudaEvent_t trace_ev[2 * kTraceEvents] = {};
     cudaEvent_t wave_ev[2] = {nullptr, nullptr};   // the last two waves of a render (bounded run-ahead)
+    static constexpr int kHostBands = 8;           // row bands a host-memory frame is shaded and copied out in
+    cudaStream_t copy_stream = nullptr;            // device-to-host copies of finished bands
+    cudaEvent_t band_ev[kHostBands] = {};
     // reusable scratch for host-pointer calls
     DevBuf scratch[4];
     MrtArena *arena = nullptr;          // device allocations of this context come from here when set
@@ -109,8 +112,19 @@ int build_grids(MrtScene *s, const float *camera_min, const float *camera_max, i
 int launch_trace_closest(MrtScene *s, const MrtRay *d_rays, uint32_t n, MrtHit *d_hits);
 int launch_trace_any(MrtScene *s, const MrtRay *d_rays, const float *d_dist, uint32_t n, uint8_t *d_occ);
 int launch_trace_counts(MrtScene *s, const MrtRay *d_rays, uint32_t n, uint32_t *d_nodes, uint32_t *d_tris);
+// Page-locked host buffers of an mrt_render call on the plain rectangle (row pitch 4 * width, the
+// block schedule = the first n_tasks pixels): a render whose shading runs in whole 16-row stripes may
+// shade them in bands and copy each band out on the context's copy stream while the next is shaded.
+// `queued` is set once any copy is on that stream (the caller must then wait for it), `rows_done`
+// once every scheduled pixel's copy is (the caller then copies nothing more).
+struct HostOut {
+    uint32_t *bitmap = nullptr;
+    float *accum = nullptr;   // host sums or nullptr
+    bool queued = false;
+    bool rows_done = false;
+};
 int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-           float *d_accum, MrtRenderStats *stats);
+           float *d_accum, MrtRenderStats *stats, HostOut *out = nullptr);
 
 mrt::DevCamera make_camera(const MrtCamera &c);
 void camera_box(const MrtCamera &c, float *mn, float *mx);

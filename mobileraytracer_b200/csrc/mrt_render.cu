@@ -195,6 +195,11 @@ struct NsTraceWork {
 #define MRT_NS_SPLIT 1
 #endif
 constexpr bool kNsSplit = MRT_NS_SPLIT != 0;
+// host-memory frames shaded in bands whose copies out overlap the shading (0: one copy at the end)
+#ifndef MRT_HOST_BANDS
+#define MRT_HOST_BANDS 1
+#endif
+constexpr bool kHostBandsOn = MRT_HOST_BANDS != 0;
 // node-phase quorum of the NoShadows traversal (coherent camera rays)
 constexpr int kNsQuorum = kCameraQuorum;
 // idle lanes that trigger a refill in the NoShadows traversal
@@ -218,8 +223,12 @@ __global__ void __launch_bounds__(128, kGridBlocksPerSm) k_ns_trace_grid(DevScen
     persistent_grid_closest(s, w, lane);
 }
 
+// shading of items j0 .. j0 + n_pix - 1 of a traced chunk: the hit of sample si of item j0 + j is
+// hits[si * hit_stride + j] (hit_stride = the chunk's item count; a band of the chunk passes the hits
+// from its first item on)
 __global__ void __launch_bounds__(128) k_ns_shade(DevScene s, RenderParams p, uint32_t first, uint32_t j0, uint32_t n_pix,
-                                                  uint32_t s0, uint32_t n_s, uint32_t tiles_x, const uint2 *__restrict__ hits) {
+                                                  uint32_t s0, uint32_t n_s, uint32_t tiles_x, const uint2 *__restrict__ hits,
+                                                  uint32_t hit_stride) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_pix; j += gridDim.x * blockDim.x) {
         const Task k = task_of(p, ns_task(p, first, j0 + j, tiles_x));
         uint32_t bm = p.bitmap[k.index];
@@ -227,7 +236,7 @@ __global__ void __launch_bounds__(128) k_ns_shade(DevScene s, RenderParams p, ui
         float4 acc = slot >= 0 ? p.accum[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         for (uint32_t si = 0; si < n_s; ++si) {
             const uint32_t sample = p.spp_offset + s0 + si;
-            const uint2 h = hits[(size_t)si * n_pix + j];
+            const uint2 h = hits[(size_t)si * hit_stride + j];
             V3 rgb{0.0f, 0.0f, 0.0f};
             if (h.y != MRT_HIT_NONE) {
                 const Stream st = make_stream(p.seed, k.y * p.width + k.x, sample, p.strata, p.constant_value);
@@ -735,7 +744,7 @@ uint32_t wave_roots_setting() {
 namespace mrt_host {
 
 static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-                       float *d_accum, MrtRenderStats *stats, uint32_t strata) {
+                       float *d_accum, MrtRenderStats *stats, uint32_t strata, HostOut *out) {
     MrtContext *ctx = s->ctx;
     cudaStream_t q = ctx->stream;
     const uint32_t stride_px = stride / 4u;
@@ -781,7 +790,7 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             one.spp = 1;
             one.spp_offset = o->spp_offset + si;
             MrtRenderStats part{};
-            st = render_impl(s, cam, &one, d_bitmap, stride, d_accum, &part, strata);
+            st = render_impl(s, cam, &one, d_bitmap, stride, d_accum, &part, strata, nullptr);
             if (st != MRT_OK) return st;
             total.rays_closest += part.rays_closest;
             total.rays_shadow += part.rays_shadow;
@@ -817,11 +826,21 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
             if (s->stop.load()) return cancelled(ctx, q);
             if ((fast || accel == MRT_ACCEL_REGULAR_GRID) && kNsSplit) {
                 // chunks of at most kNsChunk (sample, pixel) items: whole samples of up to kNsChunk pixels.
-                // (Rendering a host-memory frame in four row bands, each copied out while the next band
-                // rendered, was slower end to end on the 1080p soup frame: 1121 against 1496 Mrays/s —
-                // each shorter traversal launch pays its own tail.)
+                // A frame into page-locked host buffers that is one chunk (the plain rectangle, whole
+                // 16-row stripes) is traced in one launch and shaded in up to kHostBands bands of whole
+                // stripes, so that the copies out overlap the shading.  (Tracing it in bands as well was
+                // slower end to end on the 1080p soup frame, 1121 against 1496 Mrays/s: each shorter
+                // traversal launch pays its own tail.)
                 const uint32_t count = plan.round_count[r];
                 const uint32_t n_pix_max = std::min<uint32_t>(count, kNsChunk);
+                const uint32_t stripe = 16u * o->width;
+                uint32_t band_rows = 0;   // items per band (0: one shading launch per pass, no copies here)
+                if (kHostBandsOn && out && out->bitmap && plan.implicit && plan.round_first.size() == 1 && plan.round_first[0] == 0 &&
+                    stride == 4u * o->width && count <= kNsChunk && count % stripe == 0 && count / stripe >= 2) {
+                    const uint32_t stripes = count / stripe;
+                    const uint32_t bands = std::min<uint32_t>(stripes, MrtContext::kHostBands);
+                    band_rows = ((stripes + bands - 1) / bands) * stripe;
+                }
                 st = ensure(ctx, ctx->wave[1], sizeof(uint2) * (size_t)kNsChunk);
                 if (st != MRT_OK) return st;
                 uint2 *hits = (uint2 *)ctx->wave[1].ptr;
@@ -840,8 +859,34 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
                         cudaEventRecord(ctx->trace_ev[2 * trace_pairs + 1], q);
                         ++trace_pairs;
                         launches += 2;
-                        k_ns_shade<<<(n_pix + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0, n_pix, s0, n_s,
-                                                                        tiles_x, hits);
+                        if (!band_rows || s0 + n_s < o->spp) {
+                            k_ns_shade<<<(n_pix + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0, n_pix, s0,
+                                                                            n_s, tiles_x, hits, n_pix);
+                            continue;
+                        }
+                        // the last samples of the frame: shaded band by band, each band's rows going to
+                        // the host on the copy stream while the next band is shaded
+                        launches -= 1;
+                        for (uint32_t b0 = 0; b0 < n_pix && st == MRT_OK; b0 += band_rows) {
+                            const uint32_t nb = std::min(band_rows, n_pix - b0);
+                            const int slot = (int)(b0 / band_rows);
+                            k_ns_shade<<<(nb + 127) / 128, 128, 0, q>>>(s->dev, p, plan.round_first[r], j0 + b0, nb, s0,
+                                                                         n_s, tiles_x, hits + b0, n_pix);
+                            ++launches;
+                            st = cuda_status(ctx, cudaEventRecord(ctx->band_ev[slot], q), "band event");
+                            if (st == MRT_OK)
+                                st = cuda_status(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->band_ev[slot], 0), "band wait");
+                            if (st == MRT_OK) {
+                                out->queued = true;
+                                st = cuda_status(ctx, cudaMemcpyAsync(out->bitmap + b0, d_bitmap + b0, 4ull * nb,
+                                                                      cudaMemcpyDeviceToHost, ctx->copy_stream), "band out");
+                            }
+                            if (st == MRT_OK && out->accum && d_accum)
+                                st = cuda_status(ctx, cudaMemcpyAsync(out->accum + 4ull * b0, d_accum + 4ull * b0, 16ull * nb,
+                                                                      cudaMemcpyDeviceToHost, ctx->copy_stream), "band sums out");
+                        }
+                        if (st != MRT_OK) return st;
+                        out->rows_done = true;
                     }
                 }
             } else if (fast) {
@@ -962,11 +1007,22 @@ static int render_impl(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o
 }
 
 int render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32_t *d_bitmap, uint32_t stride,
-           float *d_accum, MrtRenderStats *stats) {
-    return render_impl(s, cam, o, d_bitmap, stride, d_accum, stats, o->spp);
+           float *d_accum, MrtRenderStats *stats, HostOut *out) {
+    return render_impl(s, cam, o, d_bitmap, stride, d_accum, stats, o->spp, out);
 }
 
 }  // namespace mrt_host
+
+// host memory that the driver has page-locked (cudaHostAlloc / cudaHostRegister): device copies into it
+// are asynchronous
+static bool page_locked(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
 
 extern "C" {
 
@@ -996,34 +1052,52 @@ int mrt_render(MrtScene *s, const MrtCamera *cam, const MrtRenderOpts *o, uint32
                        "sums 16-byte aligned");
         return MRT_ERR_ARG;
     }
+    HostOut out;
+    size_t rows_bytes = bm_bytes, acc_rows = accum ? acc_bytes : 0;   // what the render can change
     if (mem == MRT_MEM_HOST) {
         st = ensure(ctx, ctx->wave[7], acc_offset + (accum ? acc_bytes : 0));
         if (st != MRT_OK) return st;
         d_bitmap = (uint32_t *)ctx->wave[7].ptr;
         d_accum = accum ? (float *)((char *)ctx->wave[7].ptr + acc_offset) : nullptr;
-        // The first samples of a frame (spp_offset 0) on the plain rectangle (row pitch = 4 * width)
-        // replace every pixel they render without reading it: incrementalAvg with n = 1
-        // (Utils.cpp:48-70) keeps nothing of the old value.  Only the rows below the block schedule
-        // (height mod 16 of them, Renderer.cpp:20-21) then need the caller's bytes.
-        size_t in_from = 0;
-        if (o->spp_offset == 0 && stride_bytes == 4u * o->width) {
+        // On the plain rectangle (row pitch = 4 * width) the block schedule is the first n_tasks pixels,
+        // whole rows (the height mod 16 rows below it are never rendered, Renderer.cpp:20-21): only those
+        // go in and out, and the caller's other rows stay as they are.  The first samples of a frame
+        // (spp_offset 0) replace every pixel they render without reading it (incrementalAvg with n = 1
+        // keeps nothing of the old value, Utils.cpp:48-70): then no bitmap byte goes in.
+        bool plain = false;
+        if (stride_bytes == 4u * o->width) {
             const TaskPlan &plan = *cached_plan(s, o->width, o->height, o->width);
-            if (plan.n_tasks > 0 && plan.implicit) in_from = 4ull * plan.n_tasks;
+            plain = plan.n_tasks > 0 && plan.implicit;
+            if (plain) {
+                rows_bytes = 4ull * plan.n_tasks;
+                if (accum) acc_rows = 16ull * plan.n_tasks;
+            }
         }
-        if (in_from < bm_bytes)
-            st = cuda_status(ctx, cudaMemcpyAsync((char *)d_bitmap + in_from, (const char *)bitmap + in_from,
-                                                  bm_bytes - in_from, cudaMemcpyHostToDevice, ctx->stream),
-                             "bitmap in");
+        const size_t in_bytes = (plain && o->spp_offset == 0) ? 0 : rows_bytes;
+        if (in_bytes)
+            st = cuda_status(ctx, cudaMemcpyAsync(d_bitmap, bitmap, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "bitmap in");
         if (st == MRT_OK && accum)
-            st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_bytes, cudaMemcpyHostToDevice, ctx->stream), "accum in");
+            st = cuda_status(ctx, cudaMemcpyAsync(d_accum, accum, acc_rows, cudaMemcpyHostToDevice, ctx->stream), "accum in");
         if (st != MRT_OK) return st;
+        // page-locked buffers: the render may copy finished bands out while it shades the rest (a copy
+        // into pageable memory would return only when done, holding up the launches behind it)
+        if (plain && page_locked(bitmap) && (!accum || page_locked(accum))) {
+            out.bitmap = bitmap;
+            out.accum = accum;
+        }
     }
-    st = render(s, cam, o, d_bitmap, stride_bytes, d_accum, stats);
-    if (st == MRT_OK && mem == MRT_MEM_HOST) {
-        st = cuda_status(ctx, cudaMemcpyAsync(bitmap, d_bitmap, bm_bytes, cudaMemcpyDeviceToHost, ctx->stream), "bitmap out");
-        if (st == MRT_OK && accum)
-            st = cuda_status(ctx, cudaMemcpyAsync(accum, d_accum, acc_bytes, cudaMemcpyDeviceToHost, ctx->stream), "accum out");
-        if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "render copy out");
+    st = render(s, cam, o, d_bitmap, stride_bytes, d_accum, stats, out.bitmap ? &out : nullptr);
+    if (mem == MRT_MEM_HOST) {
+        if (st == MRT_OK && !out.rows_done) {
+            st = cuda_status(ctx, cudaMemcpyAsync(bitmap, d_bitmap, rows_bytes, cudaMemcpyDeviceToHost, ctx->stream), "bitmap out");
+            if (st == MRT_OK && accum)
+                st = cuda_status(ctx, cudaMemcpyAsync(accum, d_accum, acc_rows, cudaMemcpyDeviceToHost, ctx->stream), "accum out");
+            if (st == MRT_OK) st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "render copy out");
+        }
+        if (out.queued) {   // copies of bands on the copy stream: done before the call returns, also on an error
+            const int cs = cuda_status(ctx, cudaStreamSynchronize(ctx->copy_stream), "render band copies");
+            if (st == MRT_OK) st = cs;
+        }
     }
     return st;
 }

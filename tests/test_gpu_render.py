@@ -184,6 +184,42 @@ def test_host_path_trace_and_shade_equal_the_device_path(ctx):
         g.close()
 
 
+def test_page_locked_host_frames_shade_in_bands(ctx):
+    """Page-locked host buffers on the plain rectangle: the trace + shade path shades the last samples
+    in bands of whole 16-row stripes and copies each out while the next is shaded.  Bitmap and sums
+    equal the device path started from the same bytes (first passes and continuations, one and several
+    samples, FAST BVH and RegularGrid), the rows below the block schedule keep the caller's bytes, and
+    pageable buffers of the same frame give the same result in one shading launch per pass."""
+    torch = pytest.importorskip("torch")
+    soup = scenes.triangle_soup(20_000, 5, 320, 240)
+    rng = np.random.default_rng(11)
+    for accel, w, h, spp, spp_offset in ((capi.MRT_ACCEL_BVH, 320, 200, 1, 0), (capi.MRT_ACCEL_BVH, 320, 240, 3, 0),
+                                         (capi.MRT_ACCEL_REGULAR_GRID, 320, 200, 2, 1),
+                                         (capi.MRT_ACCEL_BVH, 96, 152, 2, 2)):
+        g = Scene(ctx, soup).build(accel)
+        opts = capi.render_opts(shader=NS, width=w, height=h, spp=spp, spl=1, seed=4, spp_offset=spp_offset)
+        start = rng.integers(0, 2**32, size=(h, w), dtype=np.uint32)
+        start_acc = rng.random((h, w, 4), dtype=np.float32)
+        host_bm = torch.from_numpy(start.view(np.int32).copy()).pin_memory().numpy().view(np.uint32)
+        host_acc = torch.from_numpy(start_acc.copy()).pin_memory().numpy()
+        _, _, st = g.render(soup.camera, opts, bitmap=host_bm, accum=host_acc)
+        rows = 16 * (h // 16)
+        assert st.kernel_launches > 2, (accel, w, h)   # one trace launch, several shading bands
+        dev_bm = torch.from_numpy(start.view(np.int32).copy()).cuda()
+        dev_acc = torch.from_numpy(start_acc.copy()).cuda()
+        g.render(soup.camera, opts, bitmap=dev_bm, accum=dev_acc)
+        torch.cuda.synchronize()
+        assert np.array_equal(host_bm, dev_bm.cpu().numpy().view(np.uint32)), (accel, w, h, spp)
+        assert np.array_equal(host_acc.view(np.uint32), dev_acc.cpu().numpy().view(np.uint32))
+        assert (host_bm[rows:] == start[rows:]).all() and (host_acc[rows:] == start_acc[rows:]).all()
+        pageable = start.copy()
+        pageable_acc = start_acc.copy()
+        _, _, st2 = g.render(soup.camera, opts, bitmap=pageable, accum=pageable_acc)
+        assert np.array_equal(pageable, host_bm) and np.array_equal(pageable_acc.view(np.uint32), host_acc.view(np.uint32))
+        assert st2.kernel_launches < st.kernel_launches
+        g.close()
+
+
 def test_errors_are_reported(ctx):
     import mobileraytracer_b200 as m
     sc = scenes.glass_room()
